@@ -1,0 +1,187 @@
+/*
+ * mvbt.h -- C ABI of the B200 multiversion B-link tree (libmvbt.so).
+ *
+ * Plain pointers, sizes and status codes only, so any FFI (ctypes, cgo, JNI, N-API) can bind it.
+ * Every array argument is a device pointer (or pinned, UVA-mapped host memory, as the
+ * reference's own tests pass) unless the comment says "host". `stream` is a cudaStream_t
+ * passed as void* (NULL = the legacy default stream). All operations are stream ordered and
+ * asynchronous unless stated otherwise.
+ *
+ * Each entry point names the reference interface it replaces (owensgroup/MVGpuBTree, a header-only
+ * C++ template library: GpuBTree::gpu_blink_tree and GpuBTree::gpu_versioned_btree in
+ * include/gpu_blink_tree.hpp and include/gpu_versioned_blink_tree.hpp).
+ *
+ * Keys and values are uint32. Key 0xFFFFFFFF is reserved (an empty slot); 0xFFFFFFFF as a found
+ * value is the not-found sentinel. Key 0 starts present with value 0 (the reference's root
+ * tombstone). Range queries are half-open [lower, upper).
+ */
+#ifndef MVBT_H_
+#define MVBT_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. */
+#define MVBT_OK 0
+#define MVBT_ERR_BAD_ARG 1        /* invalid argument (null handle, bad tile width, ...) */
+#define MVBT_ERR_CUDA 2           /* a CUDA runtime call failed; see mvbt_last_error() */
+#define MVBT_ERR_POOL_EXHAUSTED 3 /* the node pool is full (device error bit) */
+#define MVBT_ERR_SPIN_LIMIT 4     /* a bounded wait gave up (device error bit) */
+#define MVBT_ERR_CORRUPT 5        /* a structural invariant failed (device error bit) */
+#define MVBT_ERR_NOT_SUPPORTED 6  /* operation not available for this tree kind */
+#define MVBT_ERR_OUT_OF_MEMORY 7  /* cudaMalloc of the pool / buffers failed */
+
+/* Device error bits reported by mvbt_check_errors(). */
+#define MVBT_DEVERR_POOL_EXHAUSTED 1u
+#define MVBT_DEVERR_SPIN_LIMIT 2u
+#define MVBT_DEVERR_CORRUPT 4u
+#define MVBT_DEVERR_STEP_LIMIT 8u
+
+/* Tree kinds. */
+#define MVBT_KIND_BLINK 0     /* GpuBTree::gpu_blink_tree */
+#define MVBT_KIND_VERSIONED 1 /* GpuBTree::gpu_versioned_btree (alias gpu_versioned_blink_tree) */
+
+/* Timestamp that reads the newest version (the reference's invalid_timestamp_). */
+#define MVBT_LATEST 0xFFFFFFFFu
+#define MVBT_NOT_FOUND 0xFFFFFFFFu
+
+typedef struct mvbt_tree mvbt_tree;
+
+/* A range-query result pair; layout of the reference's pair_type<uint32,uint32>
+ * (include/pair_type.hpp:22-30). */
+typedef struct mvbt_pair {
+  uint32_t first;
+  uint32_t second;
+} mvbt_pair;
+
+typedef struct mvbt_config {
+  uint64_t pool_bytes;  /* node pool size in bytes (0 = 4 GiB); at most 2^28 nodes of 128 B */
+  int32_t device;       /* CUDA device ordinal (-1 = current device) */
+  int32_t tile_width;   /* threads per node tile for the bulk kernels: 8 or 16 (0 = 8) */
+  int32_t block_size;   /* threads per block of the bulk kernels (0 = 256) */
+  uint32_t spin_limit;  /* bounded-wait attempts before an op gives up (0 = 1<<20) */
+  uint32_t chunk_nodes; /* nodes per per-SM allocation chunk (0 = 64) */
+  uint32_t reserved[7];
+} mvbt_config;
+
+/* Structural report of a host walk over a copy of the node pool (mvbt_validate). */
+typedef struct mvbt_report {
+  uint32_t height;          /* levels, leaves included */
+  uint32_t reserved0;
+  uint64_t keys;            /* visible keys (the tombstone key 0 included if present) */
+  uint64_t leaves;          /* leaf nodes on the level-0 chain */
+  uint64_t interior;        /* interior nodes */
+  uint64_t nodes_allocated; /* nodes handed out by the allocator (all versions) */
+  uint64_t key_checksum;    /* sum over visible pairs of (key * 0x9E3779B1 + value), mod 2^64 */
+  uint32_t locked_nodes;    /* nodes left locked (must be 0 between kernels) */
+  uint32_t violations;      /* failed invariants (order, fences, levels, links) */
+} mvbt_report;
+
+/* Device view for user kernels (see include/mvbt_device.cuh: mvbt::device_tree). */
+typedef struct mvbt_device_view {
+  void* pool;         /* node array, 128 B per node */
+  void* control;      /* device control block */
+  uint32_t versioned; /* 1 = multiversion tree */
+  uint32_t capacity;  /* pool size in nodes */
+} mvbt_device_view;
+
+void mvbt_config_init(mvbt_config* cfg);
+
+/* Creates a tree with one root leaf holding the tombstone {0, 0}; synchronises the device.
+ * Replaces: gpu_blink_tree() (include/gpu_blink_tree.hpp:77-81) and gpu_versioned_btree()
+ * (include/gpu_versioned_blink_tree.hpp:88-93). */
+int mvbt_create(int kind, const mvbt_config* cfg, mvbt_tree** out);
+
+/* Frees the pool and all buffers. Replaces the shared_ptr teardown of the reference handles. */
+int mvbt_destroy(mvbt_tree* tree);
+
+/* Upserts n pairs. in_place selects the reference's ViB (1) or VoB (0) insert; both keep every
+ * version an older snapshot can read, so results are identical; blink trees ignore it.
+ * Replaces: gpu_blink_tree::insert (include/gpu_blink_tree.hpp:218-225),
+ * gpu_versioned_btree::insert(..., in_place) (include/gpu_versioned_blink_tree.hpp:106-142). */
+int mvbt_insert(mvbt_tree* tree, const uint32_t* keys, const uint32_t* values, uint32_t n,
+                void* stream, int in_place);
+
+/* values[i] = value of keys[i] at snapshot `timestamp` (MVBT_LATEST = newest), else
+ * MVBT_NOT_FOUND. concurrent = 1 when writers may run on the tree at the same time.
+ * Replaces: gpu_blink_tree::find (include/gpu_blink_tree.hpp:227-236),
+ * gpu_versioned_btree::find (include/gpu_versioned_blink_tree.hpp:144-164). */
+int mvbt_find(mvbt_tree* tree, const uint32_t* keys, uint32_t* values, uint32_t n,
+              uint32_t timestamp, void* stream, int concurrent);
+
+/* Erases n keys (missing keys are no-ops). On a versioned tree the erase is a new version, so
+ * reads at older snapshots still see the key.
+ * Replaces: gpu_blink_tree::erase (include/gpu_blink_tree.hpp:238-245),
+ * gpu_versioned_btree::erase (include/gpu_versioned_blink_tree.hpp:166-173). */
+int mvbt_erase(mvbt_tree* tree, const uint32_t* keys, uint32_t n, void* stream, int concurrent);
+
+/* Range query i returns the pairs with lower[i] <= key < upper[i], ascending, written from
+ * result + i * average_range_length; at most average_range_length pairs are written (the
+ * reference writes past the slot), counts[i] (nullable) receives the full count.
+ * Replaces: gpu_blink_tree::range_query (include/gpu_blink_tree.hpp:247-265),
+ * gpu_versioned_btree::range_query(..., timestamp, ...) (include/gpu_versioned_blink_tree.hpp:195-216). */
+int mvbt_range_query(mvbt_tree* tree, const uint32_t* lower, const uint32_t* upper,
+                     mvbt_pair* result, uint32_t* counts, uint32_t average_range_length, uint32_t n,
+                     uint32_t timestamp, void* stream, int concurrent);
+
+/* One kernel mixing n_insert inserts with n_range range queries. A snapshot S is taken when the
+ * call is issued; every range query reads at S and every insert lands after it, so results are
+ * deterministic. counts (nullable) receives each query's full count.
+ * Replaces: concurrent_insert_range (include/gpu_blink_tree.hpp:148-187,
+ * include/gpu_versioned_blink_tree.hpp:252-294). */
+int mvbt_concurrent_insert_range(mvbt_tree* tree, const uint32_t* keys, const uint32_t* values,
+                                 uint32_t n_insert, const uint32_t* lower, const uint32_t* upper,
+                                 uint32_t n_range, mvbt_pair* result,
+                                 uint32_t average_range_length, uint32_t* counts, void* stream);
+
+/* One kernel mixing n_find finds with n_erase erases; finds read at a snapshot taken when the
+ * call is issued (versioned tree) or the newest state (blink tree).
+ * Replaces: concurrent_find_erase (include/gpu_blink_tree.hpp:189-216,
+ * include/gpu_versioned_blink_tree.hpp:218-250). */
+int mvbt_concurrent_find_erase(mvbt_tree* tree, const uint32_t* find_keys, uint32_t* find_results,
+                               uint32_t n_find, const uint32_t* erase_keys, uint32_t n_erase,
+                               void* stream);
+
+/* Takes a snapshot and returns its id in *snapshot_out (host); synchronises `stream`.
+ * Replaces: gpu_versioned_btree::take_snapshot (include/gpu_versioned_blink_tree.hpp:297-302). */
+int mvbt_take_snapshot(mvbt_tree* tree, void* stream, uint32_t* snapshot_out);
+
+/* Stream-ordered snapshot: writes the id to the device word d_snapshot_out, no host sync. */
+int mvbt_take_snapshot_async(mvbt_tree* tree, void* stream, uint32_t* d_snapshot_out);
+
+/* Synchronises `stream` and returns the sticky device error bits (MVBT_DEVERR_*) in *bits;
+ * the status is MVBT_OK when no bit is set, else the first matching MVBT_ERR_*. */
+int mvbt_check_errors(mvbt_tree* tree, void* stream, uint32_t* bits);
+
+/* Clears the sticky device error bits. */
+int mvbt_clear_errors(mvbt_tree* tree, void* stream);
+
+/* Allocator usage. Replaces: compute_memory_usage (include/gpu_blink_tree.hpp:1076-1080). */
+int mvbt_memory_usage(mvbt_tree* tree, uint64_t* nodes_allocated, uint64_t* bytes_allocated,
+                      uint64_t* pool_bytes);
+
+/* Host walk of the tree as visible at `timestamp`: checks key order, fences, levels, links and
+ * lock bits and fills *report. Synchronises the device.
+ * Replaces: validate_tree_structure (include/gpu_blink_tree.hpp:742-900,
+ * include/gpu_versioned_blink_tree.hpp:1098-1259). */
+int mvbt_validate(mvbt_tree* tree, uint32_t timestamp, mvbt_report* report);
+
+/* Device view for user kernels calling the cooperative_* device API. */
+int mvbt_get_device_view(mvbt_tree* tree, mvbt_device_view* out);
+
+/* Tree kind, tile width and device of a handle. */
+int mvbt_get_info(mvbt_tree* tree, int* kind, int* tile_width, int* device);
+
+/* Last error message of this thread (host-side detail for MVBT_ERR_CUDA / BAD_ARG). */
+const char* mvbt_last_error(void);
+const char* mvbt_status_string(int status);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MVBT_H_ */

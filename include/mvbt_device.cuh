@@ -1,0 +1,911 @@
+// Device-side multiversion B-link tree for sm_100a.
+//
+// This header is the device half of the library. Its kernels (mvgpubtree_b200/csrc) and user
+// kernels call the same tile-cooperative operations, the counterparts of the reference's
+// device methods:
+//   cooperative_find          <- gpu_blink_tree::cooperative_find (include/gpu_blink_tree.hpp:277-303)
+//                                gpu_versioned_btree::cooperative_find(key, tile, alloc, ts, ...)
+//                                (include/gpu_versioned_blink_tree.hpp:438-474)
+//   cooperative_insert        <- cooperative_insert_blink (include/gpu_blink_tree.hpp:522-733) and
+//                                cooperative_insert_versioned_in_place
+//                                (include/gpu_versioned_blink_tree.hpp:824-1086)
+//   cooperative_erase         <- cooperative_erase (include/gpu_blink_tree.hpp:357-390,
+//                                include/gpu_versioned_blink_tree.hpp:393-436)
+//   cooperative_range_query   <- cooperative_range_query (include/gpu_blink_tree.hpp:306-355) and
+//                                concurrent_cooperative_range_query
+//                                (include/gpu_versioned_blink_tree.hpp:504-559)
+//   take_snapshot             <- take_snapshot(tile) (include/gpu_versioned_blink_tree.hpp:332-344)
+//
+// Node format (128 bytes, 128-byte aligned, 32 words):
+//   pairs 0..13  {key, value}  leaf: key/value, interior: {separator, child index}; sorted by key,
+//                              unused pairs are {0xFFFFFFFF, 0xFFFFFFFF}
+//   pair 14      {high key, link}     high key = exclusive upper fence (0xFFFFFFFF on the
+//                                     rightmost node of a level); link = bit31 lock |
+//                                     bits 0..27 right-sibling index (0x0FFFFFFF = none)
+//   pair 15      {ts, older|level}    ts = epoch of this version; bits 28..31 level (0 = leaf),
+//                                     bits 0..27 index of the next older version (none = 0x0FFFFFFF)
+// A tile of W threads (W = 8 or 16) holds one node in registers: lane l owns pairs
+// [l*16/W, (l+1)*16/W), so an 8-lane tile reads a node as eight 16-byte vector loads and a
+// 16-lane tile as sixteen 8-byte loads -- one 128-byte line either way.
+//
+// Concurrency protocol (B-link, Lehman-Yao style):
+//   * readers never lock; a reader whose key is >= a node's high key follows the right link;
+//   * a writer locks one leaf (atomicOr on the lock bit, bounded spin with __nanosleep backoff),
+//     moves right under lock coupling, and applies its change; a full node splits into itself
+//     and a new right sibling (right written first, then left, each followed by a fence), then
+//     the writer releases the node and inserts the separator into the parent recorded on its
+//     way down (moving right there as needed); the root keeps index 0 and grows by copying its
+//     halves into two new children;
+//   * versioning (versioned trees): a writer in epoch E that first touches a node whose ts < E
+//     copies it to a fresh node O, publishes the header {ts = E, older = O} before changing the
+//     data, and nodes created by splits in epoch E point to the same O. A reader at snapshot S
+//     follows `older` while ts > S, so the version it uses is immutable.
+//   * every wait is bounded; on a limit the operation gives up, records an error bit in the
+//     control block and returns (no trap, no unbounded loop).
+#pragma once
+
+#include <cooperative_groups.h>
+#include <cstdint>
+
+#ifndef MVBT_DEV
+#define MVBT_DEV __device__ __forceinline__
+#endif
+
+namespace mvbt {
+namespace cg = cooperative_groups;
+
+// ----------------------------------------------------------------------------------------------
+// Constants
+// ----------------------------------------------------------------------------------------------
+constexpr int kNodeWords      = 32;
+constexpr int kDataPairs      = 14;
+constexpr int kSplitLeft      = 8;  // a full node plus one entry (15) splits 8 | 7
+constexpr uint32_t kEmptyKey  = 0xFFFFFFFFu;
+constexpr uint32_t kNotFound  = 0xFFFFFFFFu;
+constexpr uint32_t kLatest    = 0xFFFFFFFFu;  // read the newest version
+constexpr uint32_t kNone      = 0x0FFFFFFFu;  // "no node" in 28-bit index fields
+constexpr uint32_t kIndexMask = 0x0FFFFFFFu;
+constexpr uint32_t kLockBit   = 0x80000000u;
+constexpr uint32_t kRoot      = 0;
+constexpr int kMaxLevels      = 16;
+constexpr int kMaxSmSlots     = 256;
+constexpr uint32_t kMaxSteps  = 1u << 16;  // node visits per operation before giving up
+
+// Sticky error bits in control_block::error.
+enum : uint32_t {
+  kErrPoolExhausted = 1u,
+  kErrSpinLimit     = 2u,
+  kErrCorrupt       = 4u,
+  kErrStepLimit     = 8u,
+};
+
+// Device-resident tree state (one per tree).
+struct control_block {
+  uint32_t epoch;       // current write epoch == id the next take_snapshot returns
+  uint32_t error;       // sticky error bits
+  uint32_t bump;        // first never-allocated node index
+  uint32_t capacity;    // pool capacity in nodes
+  uint32_t chunk;       // nodes per per-SM allocation chunk
+  uint32_t spin_limit;  // lock / wait attempts before giving up
+  uint32_t wait_ns;     // wall-clock limit of one bounded wait (ns)
+  uint32_t reserved;
+  unsigned long long stat_cow;    // copy-on-write versions created
+  unsigned long long stat_split;  // node splits
+  unsigned long long stat_restart;
+  unsigned long long stat_reserved;
+  unsigned long long sm_pool[kMaxSmSlots];  // per-SM chunk cursor: (base << 32) | used
+};
+
+// ----------------------------------------------------------------------------------------------
+// Low-level memory access
+// ----------------------------------------------------------------------------------------------
+template <int W>
+struct node_regs {
+  static constexpr int P = 16 / W;  // pairs per lane
+  uint32_t k[P];
+  uint32_t v[P];
+};
+
+MVBT_DEV uint32_t sm_id() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%smid;" : "=r"(r));
+  return r;
+}
+
+MVBT_DEV unsigned long long global_ns() {
+  unsigned long long r;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(r));
+  return r;
+}
+
+MVBT_DEV uint32_t ld_relaxed_u32(const uint32_t* p) {
+  uint32_t r;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(r) : "l"(p) : "memory");
+  return r;
+}
+MVBT_DEV unsigned long long ld_relaxed_u64(const unsigned long long* p) {
+  unsigned long long r;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(r) : "l"(p) : "memory");
+  return r;
+}
+
+// Loads this lane's share of a node. strong = L2-coherent relaxed loads (needed while writers
+// may run in the same kernel); otherwise read-only cached loads.
+template <int W>
+MVBT_DEV void ld_lane(const uint32_t* p, node_regs<W>& n, bool strong) {
+  if constexpr (W == 8) {
+    if (strong) {
+      asm volatile("ld.relaxed.gpu.global.v4.u32 {%0,%1,%2,%3}, [%4];"
+                   : "=r"(n.k[0]), "=r"(n.v[0]), "=r"(n.k[1]), "=r"(n.v[1])
+                   : "l"(p)
+                   : "memory");
+    } else {
+      asm("ld.global.nc.v4.u32 {%0,%1,%2,%3}, [%4];"
+          : "=r"(n.k[0]), "=r"(n.v[0]), "=r"(n.k[1]), "=r"(n.v[1])
+          : "l"(p));
+    }
+  } else {
+    if (strong) {
+      asm volatile("ld.relaxed.gpu.global.v2.u32 {%0,%1}, [%2];"
+                   : "=r"(n.k[0]), "=r"(n.v[0])
+                   : "l"(p)
+                   : "memory");
+    } else {
+      asm("ld.global.nc.v2.u32 {%0,%1}, [%2];" : "=r"(n.k[0]), "=r"(n.v[0]) : "l"(p));
+    }
+  }
+}
+
+template <int W>
+MVBT_DEV void st_lane(uint32_t* p, const node_regs<W>& n) {
+  if constexpr (W == 8) {
+    asm volatile("st.relaxed.gpu.global.v4.u32 [%0], {%1,%2,%3,%4};"
+                 :
+                 : "l"(p), "r"(n.k[0]), "r"(n.v[0]), "r"(n.k[1]), "r"(n.v[1])
+                 : "memory");
+  } else {
+    asm volatile("st.relaxed.gpu.global.v2.u32 [%0], {%1,%2};"
+                 :
+                 : "l"(p), "r"(n.k[0]), "r"(n.v[0])
+                 : "memory");
+  }
+}
+
+// ----------------------------------------------------------------------------------------------
+// Register-resident node helpers (all are tile-collective: every lane must call them)
+// ----------------------------------------------------------------------------------------------
+template <int W>
+struct layout {
+  static constexpr int P          = 16 / W;
+  static constexpr int kLinkLane  = 14 / P;  // lane owning pair 14 {high, link}
+  static constexpr int kLinkSlot  = 14 % P;
+  static constexpr int kVerLane   = 15 / P;  // lane owning pair 15 {ts, older|level}
+  static constexpr int kVerSlot   = 15 % P;
+};
+
+struct header {
+  uint32_t high;
+  uint32_t link;
+  uint32_t ts;
+  uint32_t ol;  // older | level << 28
+  MVBT_DEV uint32_t level() const { return ol >> 28; }
+  MVBT_DEV uint32_t older() const { return ol & kIndexMask; }
+  MVBT_DEV uint32_t sibling() const { return link & kIndexMask; }
+  MVBT_DEV bool is_leaf() const { return level() == 0; }
+};
+
+template <int W, class Tile>
+MVBT_DEV header get_header(const node_regs<W>& n, const Tile& t) {
+  using L = layout<W>;
+  header h;
+  h.high = t.shfl(n.k[L::kLinkSlot], L::kLinkLane);
+  h.link = t.shfl(n.v[L::kLinkSlot], L::kLinkLane);
+  h.ts   = t.shfl(n.k[L::kVerSlot], L::kVerLane);
+  h.ol   = t.shfl(n.v[L::kVerSlot], L::kVerLane);
+  return h;
+}
+
+template <int W, class Tile>
+MVBT_DEV void set_header(node_regs<W>& n, const header& h, const Tile& t) {
+  using L      = layout<W>;
+  const int r  = t.thread_rank();
+  if (r == L::kLinkLane) {
+    n.k[L::kLinkSlot] = h.high;
+    n.v[L::kLinkSlot] = h.link;
+  }
+  if (r == L::kVerLane) {
+    n.k[L::kVerSlot] = h.ts;
+    n.v[L::kVerSlot] = h.ol;
+  }
+}
+
+// Pair index of slot j in this lane.
+template <int W, class Tile>
+MVBT_DEV int pair_index(const Tile& t, int j) {
+  return t.thread_rank() * (16 / W) + j;
+}
+
+// Number of valid data pairs.
+template <int W, class Tile>
+MVBT_DEV int count_valid(const node_regs<W>& n, const Tile& t) {
+  int c = 0;
+#pragma unroll
+  for (int j = 0; j < 16 / W; ++j) {
+    bool valid = pair_index<W>(t, j) < kDataPairs && n.k[j] != kEmptyKey;
+    c += __popc(t.ballot(valid));
+  }
+  return c;
+}
+
+// Number of valid data pairs whose key is < key (= insertion position).
+template <int W, class Tile>
+MVBT_DEV int count_less(const node_regs<W>& n, uint32_t key, const Tile& t) {
+  int c = 0;
+#pragma unroll
+  for (int j = 0; j < 16 / W; ++j) {
+    bool less = pair_index<W>(t, j) < kDataPairs && n.k[j] != kEmptyKey && n.k[j] < key;
+    c += __popc(t.ballot(less));
+  }
+  return c;
+}
+
+// Interior search: child of the last pair whose separator is <= key. Returns kNone if no
+// separator is <= key (only possible on a corrupt route).
+template <int W, class Tile>
+MVBT_DEV uint32_t child_for(const node_regs<W>& n, uint32_t key, const Tile& t) {
+  constexpr int P = 16 / W;
+  int cnt         = 0;
+#pragma unroll
+  for (int j = 0; j < P; ++j) {
+    bool le = pair_index<W>(t, j) < kDataPairs && n.k[j] != kEmptyKey && n.k[j] <= key;
+    cnt += le ? 1 : 0;
+  }
+  uint32_t mask = t.ballot(cnt > 0);
+  uint32_t cand = n.v[0];
+  if constexpr (P == 2) cand = (cnt == 2) ? n.v[1] : n.v[0];
+  int src        = mask ? (31 - __clz(mask)) : 0;
+  uint32_t child = t.shfl(cand, src);
+  return mask ? child : kNone;
+}
+
+// Leaf search: value stored for key, or kNotFound.
+template <int W, class Tile>
+MVBT_DEV uint32_t leaf_value(const node_regs<W>& n, uint32_t key, const Tile& t) {
+  constexpr int P = 16 / W;
+  bool hit        = false;
+  uint32_t val    = kNotFound;
+#pragma unroll
+  for (int j = 0; j < P; ++j) {
+    if (pair_index<W>(t, j) < kDataPairs && n.k[j] == key) {
+      hit = true;
+      val = n.v[j];
+    }
+  }
+  uint32_t mask = t.ballot(hit);
+  uint32_t r    = t.shfl(val, mask ? (__ffs(mask) - 1) : 0);
+  return (mask && key != kEmptyKey) ? r : kNotFound;
+}
+
+// Fetches pair `src` (per-lane index, 0..15) of node n. Collective.
+template <int W, class Tile>
+MVBT_DEV void fetch_pair(const node_regs<W>& n, int src, uint32_t& k, uint32_t& v, const Tile& t) {
+  constexpr int P = 16 / W;
+  src             = src < 0 ? 0 : (src > 15 ? 15 : src);
+  if constexpr (P == 1) {
+    k = t.shfl(n.k[0], src);
+    v = t.shfl(n.v[0], src);
+  } else {
+    int lane    = src >> 1;
+    uint32_t k0 = t.shfl(n.k[0], lane), k1 = t.shfl(n.k[1], lane);
+    uint32_t v0 = t.shfl(n.v[0], lane), v1 = t.shfl(n.v[1], lane);
+    k           = (src & 1) ? k1 : k0;
+    v           = (src & 1) ? v1 : v0;
+  }
+}
+
+// Data pairs of the merged sequence "n's valid pairs with {key, val} inserted at pos":
+// entry e < pos -> old e, e == pos -> new, e > pos -> old e - 1. Entries past `total` are empty.
+// Output pair q of `out` takes merged entry q + first (q < take), else empty. Header pairs of
+// `out` are copied from n.
+template <int W, class Tile>
+MVBT_DEV void build_from_merged(const node_regs<W>& n,
+                                int pos,
+                                uint32_t key,
+                                uint32_t val,
+                                int first,
+                                int take,
+                                node_regs<W>& out,
+                                const Tile& t) {
+  constexpr int P = 16 / W;
+#pragma unroll
+  for (int j = 0; j < P; ++j) {
+    const int q = pair_index<W>(t, j);
+    const int e = q + first;
+    int src     = (e < pos) ? e : e - 1;
+    uint32_t fk, fv;
+    fetch_pair<W>(n, src, fk, fv, t);
+    if (q >= kDataPairs) {
+      out.k[j] = n.k[j];
+      out.v[j] = n.v[j];
+    } else if (q >= take) {
+      out.k[j] = kEmptyKey;
+      out.v[j] = kEmptyKey;
+    } else if (e == pos) {
+      out.k[j] = key;
+      out.v[j] = val;
+    } else {
+      out.k[j] = fk;
+      out.v[j] = fv;
+    }
+  }
+}
+
+// Removes data pair pos (shifting the rest down).
+template <int W, class Tile>
+MVBT_DEV void remove_at(node_regs<W>& n, int pos, const Tile& t) {
+  constexpr int P = 16 / W;
+  node_regs<W> out;
+#pragma unroll
+  for (int j = 0; j < P; ++j) {
+    const int q = pair_index<W>(t, j);
+    int src     = (q < pos) ? q : q + 1;
+    uint32_t fk, fv;
+    fetch_pair<W>(n, src, fk, fv, t);
+    if (q >= kDataPairs) {
+      out.k[j] = n.k[j];
+      out.v[j] = n.v[j];
+    } else if (src >= kDataPairs) {
+      out.k[j] = kEmptyKey;
+      out.v[j] = kEmptyKey;
+    } else {
+      out.k[j] = fk;
+      out.v[j] = fv;
+    }
+  }
+  n = out;
+}
+
+// Pair index of the data pair holding key, or -1.
+template <int W, class Tile>
+MVBT_DEV int find_pos(const node_regs<W>& n, uint32_t key, const Tile& t) {
+  constexpr int P = 16 / W;
+  int pos         = -1;
+#pragma unroll
+  for (int j = 0; j < P; ++j) {
+    uint32_t mask = t.ballot(pair_index<W>(t, j) < kDataPairs && n.k[j] == key);
+    int p         = mask ? (__ffs(mask) - 1) * P + j : -1;
+    pos           = (pos < 0) ? p : ((p >= 0 && p < pos) ? p : pos);
+  }
+  return key == kEmptyKey ? -1 : pos;
+}
+
+// ----------------------------------------------------------------------------------------------
+// The tree view: a plain struct passed to kernels by value.
+// ----------------------------------------------------------------------------------------------
+struct device_tree {
+  uint32_t* pool;       // node words; node i starts at pool + 32 * i
+  control_block* ctl;   // device control block
+  uint32_t versioned;   // 1 = multiversion tree, 0 = plain B-link tree
+  uint32_t capacity;    // pool size in nodes: every index read from memory is checked against it
+
+  MVBT_DEV uint32_t* node_ptr(uint32_t idx) const { return pool + (size_t)idx * kNodeWords; }
+  // An index is dereferenced only after this check; a bad one records kErrCorrupt instead.
+  template <class Tile>
+  MVBT_DEV bool valid(uint32_t idx, const Tile& t) const {
+    if (idx < capacity) return true;
+    if (t.thread_rank() == 0) set_error(kErrCorrupt);
+    return false;
+  }
+
+  template <int W, class Tile>
+  MVBT_DEV void load(uint32_t idx, node_regs<W>& n, bool strong, const Tile& t) const {
+    ld_lane<W>(node_ptr(idx) + t.thread_rank() * (32 / W), n, strong);
+  }
+  template <int W, class Tile>
+  MVBT_DEV void store(uint32_t idx, const node_regs<W>& n, const Tile& t) const {
+    st_lane<W>(node_ptr(idx) + t.thread_rank() * (32 / W), n);
+  }
+  // Stores only the lanes that own header pairs.
+  template <int W, class Tile>
+  MVBT_DEV void store_header(uint32_t idx, const node_regs<W>& n, const Tile& t) const {
+    using L     = layout<W>;
+    const int r = t.thread_rank();
+    if (r == L::kLinkLane || r == L::kVerLane) st_lane<W>(node_ptr(idx) + r * (32 / W), n);
+  }
+
+  MVBT_DEV void set_error(uint32_t bits) const { atomicOr(&ctl->error, bits); }
+  MVBT_DEV uint32_t current_epoch() const { return ld_relaxed_u32(&ctl->epoch); }
+
+  // ---- allocation: per-SM chunks carved from a global bump pointer ----
+  MVBT_DEV uint32_t alloc_one() const {
+    control_block* c              = ctl;
+    unsigned long long* slot      = &c->sm_pool[sm_id() % kMaxSmSlots];
+    const uint32_t C              = c->chunk;
+    const uint32_t limit          = c->spin_limit;
+    const unsigned long long t0 = global_ns();
+    for (uint32_t tries = 0; tries < limit; ++tries) {
+      if (ld_relaxed_u32(&c->error) & kErrPoolExhausted) return kNone;
+      unsigned long long old = atomicAdd(slot, 1ull);
+      uint32_t base = (uint32_t)(old >> 32), used = (uint32_t)old;
+      if (used < C) return base + used;
+      if (used == C) {  // this thread refills the chunk
+        uint32_t nb = atomicAdd(&c->bump, C);
+        if ((unsigned long long)nb + C > c->capacity) {
+          atomicOr(&c->error, kErrPoolExhausted);
+          return kNone;
+        }
+        atomicExch(slot, ((unsigned long long)nb << 32) | 1ull);
+        return nb;
+      }
+      // another thread is refilling: wait (bounded) for the chunk base to change
+      for (uint32_t w = 0; w < limit; ++w) {
+        __nanosleep(64);
+        unsigned long long cur = ld_relaxed_u64(slot);
+        if ((uint32_t)(cur >> 32) != base || (uint32_t)cur < C) break;
+        if (ld_relaxed_u32(&c->error) & kErrPoolExhausted) return kNone;
+        if (global_ns() - t0 > c->wait_ns) break;
+      }
+      if (global_ns() - t0 > c->wait_ns) break;
+    }
+    atomicOr(&c->error, kErrSpinLimit);
+    return kNone;
+  }
+  template <class Tile>
+  MVBT_DEV uint32_t alloc(const Tile& t) const {
+    uint32_t idx = kNone;
+    if (t.thread_rank() == 0) idx = alloc_one();
+    return t.shfl(idx, 0);
+  }
+
+  // ---- locks on the link word ----
+  template <class Tile>
+  MVBT_DEV bool lock(uint32_t idx, const Tile& t) const {
+    if (!valid(idx, t)) return false;
+    uint32_t* word               = node_ptr(idx) + 29;
+    uint32_t backoff             = 32;
+    const uint32_t lim           = ctl->spin_limit;
+    const unsigned long long t0  = global_ns();
+    const unsigned long long lns = ctl->wait_ns;
+    for (uint32_t i = 0; i < lim; ++i) {
+      uint32_t old = 0;
+      if (t.thread_rank() == 0) old = atomicOr(word, kLockBit);
+      old = t.shfl(old, 0);
+      if (!(old & kLockBit)) {
+        __threadfence();
+        t.sync();
+        return true;
+      }
+      // wait until the lock looks free before the next atomic
+      for (uint32_t w = 0; w < 64; ++w) {
+        __nanosleep(backoff);
+        uint32_t cur = 0;
+        if (t.thread_rank() == 0) cur = ld_relaxed_u32(word);
+        cur = t.shfl(cur, 0);
+        if (!(cur & kLockBit)) break;
+        backoff = backoff < 1024 ? backoff * 2 : 1024;
+      }
+      if (global_ns() - t0 > lns) break;
+    }
+    if (t.thread_rank() == 0) set_error(kErrSpinLimit);
+    return false;
+  }
+  template <class Tile>
+  MVBT_DEV void unlock(uint32_t idx, const Tile& t) const {
+    __threadfence();
+    t.sync();
+    if (t.thread_rank() == 0) atomicAnd(node_ptr(idx) + 29, ~kLockBit);
+  }
+
+  // ---- versioning ----
+  // Makes the version visible to older snapshots immutable before node idx (locked, content n)
+  // is changed in epoch E: copies n to a fresh node and publishes {ts = E, older = copy}.
+  template <int W, class Tile>
+  MVBT_DEV bool prepare_write(uint32_t idx, node_regs<W>& n, header& h, uint32_t E, const Tile& t) const {
+    if (!versioned || h.ts == E) return true;
+    uint32_t copy = alloc(t);
+    if (copy == kNone) return false;
+    node_regs<W> c = n;
+    header hc      = h;
+    hc.link &= ~kLockBit;
+    set_header<W>(c, hc, t);
+    store<W>(copy, c, t);
+    __threadfence();
+    h.ts = E;
+    h.ol = (h.ol & ~kIndexMask) | copy;
+    set_header<W>(n, h, t);
+    store_header<W>(idx, n, t);
+    __threadfence();
+    if (t.thread_rank() == 0) atomicAdd(&ctl->stat_cow, 1ull);
+    return true;
+  }
+
+  // Moves from node idx to the version visible at ts (snapshot readers only).
+  template <int W, class Tile>
+  MVBT_DEV bool to_version(uint32_t& idx, node_regs<W>& n, header& h, uint32_t ts, bool strong,
+                           const Tile& t) const {
+    uint32_t hops = 0;
+    while (h.ts > ts) {
+      uint32_t older = h.older();
+      if (older == kNone || ++hops > kMaxSteps) {
+        if (t.thread_rank() == 0) set_error(kErrCorrupt);
+        return false;
+      }
+      idx = older;
+      if (!valid(idx, t)) return false;
+      load<W>(idx, n, strong, t);
+      h = get_header<W>(n, t);
+    }
+    return true;
+  }
+
+  // ------------------------------------------------------------------------------------------
+  // Point lookup at snapshot ts (kLatest = newest). concurrent = writers may run meanwhile.
+  // ------------------------------------------------------------------------------------------
+  template <int W, class Tile>
+  MVBT_DEV uint32_t cooperative_find(uint32_t key, const Tile& t, uint32_t ts = kLatest,
+                                     bool concurrent = false) const {
+    const bool snap = versioned && ts != kLatest;
+    uint32_t idx    = kRoot;
+    node_regs<W> n;
+    for (uint32_t step = 0; step < kMaxSteps; ++step) {
+      if (!valid(idx, t)) return kNotFound;
+      load<W>(idx, n, concurrent, t);
+      header h = get_header<W>(n, t);
+      if (snap && !to_version<W>(idx, n, h, ts, concurrent, t)) return kNotFound;
+      if (key >= h.high && h.sibling() != kNone) {
+        idx = h.sibling();
+        continue;
+      }
+      if (h.is_leaf()) return leaf_value<W>(n, key, t);
+      idx = child_for<W>(n, key, t);
+    }
+    if (t.thread_rank() == 0) set_error(kErrStepLimit);
+    return kNotFound;
+  }
+
+  // ------------------------------------------------------------------------------------------
+  // Range query [lo, hi) at snapshot ts. Writes at most cap pairs {key, value} ascending at out
+  // (nullable) and returns the full count.
+  // ------------------------------------------------------------------------------------------
+  template <int W, class Tile>
+  MVBT_DEV uint32_t cooperative_range_query(uint32_t lo, uint32_t hi, const Tile& t, uint32_t ts,
+                                            uint2* out, uint32_t cap, bool concurrent = false) const {
+    constexpr int P = 16 / W;
+    if (hi <= lo) return 0;
+    const bool snap = versioned && ts != kLatest;
+    uint32_t idx    = kRoot;
+    node_regs<W> n;
+    header h;
+    uint32_t step = 0;
+    // descend to the leaf that holds lo
+    for (;; ++step) {
+      if (step >= kMaxSteps) {
+        if (t.thread_rank() == 0) set_error(kErrStepLimit);
+        return 0;
+      }
+      if (!valid(idx, t)) return 0;
+      load<W>(idx, n, concurrent, t);
+      h = get_header<W>(n, t);
+      if (snap && !to_version<W>(idx, n, h, ts, concurrent, t)) return 0;
+      if (lo >= h.high && h.sibling() != kNone) {
+        idx = h.sibling();
+        continue;
+      }
+      if (h.is_leaf()) break;
+      idx = child_for<W>(n, lo, t);
+    }
+    // scan leaves to the right (a sibling chain is never longer than the pool)
+    uint32_t count = 0;
+    for (uint32_t leaves = 0;; ++leaves) {
+      int first = -1, inr = 0;
+      bool in[P];
+#pragma unroll
+      for (int j = 0; j < P; ++j) {
+        int q = pair_index<W>(t, j);
+        in[j] = q < kDataPairs && n.k[j] != kEmptyKey && n.k[j] >= lo && n.k[j] < hi;
+        uint32_t m = t.ballot(in[j]);
+        inr += __popc(m);
+        if (m) {
+          int f = (__ffs(m) - 1) * P + j;
+          first = (first < 0 || f < first) ? f : first;
+        }
+      }
+      if (out != nullptr) {
+#pragma unroll
+        for (int j = 0; j < P; ++j) {
+          if (in[j]) {
+            uint32_t o = count + (uint32_t)(pair_index<W>(t, j) - first);
+            if (o < cap) out[o] = make_uint2(n.k[j], n.v[j]);
+          }
+        }
+      }
+      count += inr;
+      if (!(hi > h.high && h.sibling() != kNone)) break;
+      if (leaves >= capacity) {
+        if (t.thread_rank() == 0) set_error(kErrStepLimit);
+        break;
+      }
+      idx = h.sibling();
+      if (!valid(idx, t)) break;
+      load<W>(idx, n, concurrent, t);
+      h = get_header<W>(n, t);
+      if (snap && !to_version<W>(idx, n, h, ts, concurrent, t)) break;
+    }
+    return count;
+  }
+
+  // ------------------------------------------------------------------------------------------
+  // Writers
+  // ------------------------------------------------------------------------------------------
+  // Descends to the leaf for key (newest versions, strong loads), recording in `path` the
+  // interior node visited at each level: lane l holds level l in path0 and level l + W in path1.
+  template <int W, class Tile>
+  MVBT_DEV uint32_t descend_for_write(uint32_t key, uint32_t& path0, uint32_t& path1,
+                                      uint32_t& top_level, const Tile& t) const {
+    uint32_t idx = kRoot;
+    node_regs<W> n;
+    top_level = 0;
+    bool first = true;
+    for (uint32_t step = 0; step < kMaxSteps; ++step) {
+      if (!valid(idx, t)) return kNone;
+      load<W>(idx, n, true, t);
+      header h = get_header<W>(n, t);
+      if (first) {
+        top_level = h.level();
+        first     = false;
+      }
+      if (key >= h.high && h.sibling() != kNone) {
+        idx = h.sibling();
+        continue;
+      }
+      uint32_t lvl = h.level();
+      if (lvl == 0) return idx;
+      if (lvl < (uint32_t)W) {
+        if (t.thread_rank() == (int)lvl) path0 = idx;
+      } else {
+        if (t.thread_rank() == (int)(lvl - W)) path1 = idx;
+      }
+      idx = child_for<W>(n, key, t);
+    }
+    if (t.thread_rank() == 0) set_error(kErrStepLimit);
+    return kNone;
+  }
+
+  // Locks the node at `level` that covers key, starting from `idx` (a node at level >= level
+  // on the right path, typically the recorded parent). Returns the locked index, with n/h
+  // loaded; kNone on failure.
+  template <int W, class Tile>
+  MVBT_DEV uint32_t lock_covering(uint32_t idx, uint32_t level, uint32_t key, node_regs<W>& n,
+                                  header& h, const Tile& t) const {
+    for (uint32_t step = 0; step < kMaxSteps; ++step) {
+      if (!lock(idx, t)) return kNone;
+      load<W>(idx, n, true, t);
+      h = get_header<W>(n, t);
+      if (h.level() != level) {
+        unlock(idx, t);
+        if (h.level() < level) {
+          // The root is the only node whose level changes, and it only grows; a lower level
+          // here means the caller's route is broken.
+          if (t.thread_rank() == 0) set_error(kErrCorrupt);
+          return kNone;
+        }
+        // The tree grew above this node: walk down (unlocked) to `level` along key.
+        for (uint32_t s2 = 0; s2 < kMaxSteps && h.level() > level; ++s2) {
+          if (key >= h.high && h.sibling() != kNone) {
+            idx = h.sibling();
+          } else {
+            idx = child_for<W>(n, key, t);
+          }
+          if (!valid(idx, t)) return kNone;
+          load<W>(idx, n, true, t);
+          h = get_header<W>(n, t);
+        }
+        continue;
+      }
+      // Move right under lock coupling while key belongs further right.
+      uint32_t hops = 0;
+      while (key >= h.high && h.sibling() != kNone) {
+        uint32_t sib = h.sibling();
+        if (!lock(sib, t)) {
+          unlock(idx, t);
+          return kNone;
+        }
+        unlock(idx, t);
+        idx = sib;
+        load<W>(idx, n, true, t);
+        h = get_header<W>(n, t);
+        if (++hops > kMaxSteps) {
+          unlock(idx, t);
+          if (t.thread_rank() == 0) set_error(kErrStepLimit);
+          return kNone;
+        }
+      }
+      return idx;
+    }
+    if (t.thread_rank() == 0) set_error(kErrStepLimit);
+    return kNone;
+  }
+
+  // Splits locked node idx (content n, header h, already prepared for epoch E) while inserting
+  // {key, val}. The left half stays in idx, the right half goes to a new node. For the root the
+  // two halves go to two new children and the root becomes their parent. Outputs the separator
+  // and new right node to insert into the parent (sep_child = kNone when the root was split).
+  // The lock on idx is released.
+  template <int W, class Tile>
+  MVBT_DEV bool split_insert(uint32_t idx, node_regs<W>& n, header& h, uint32_t key, uint32_t val,
+                             uint32_t E, uint32_t& sep_key, uint32_t& sep_child, const Tile& t) const {
+    const int pos = count_less<W>(n, key, t);
+    const uint32_t ts = versioned ? E : 0u;
+    if (idx == kRoot) {
+      uint32_t a = alloc(t);
+      uint32_t b = (a == kNone) ? kNone : alloc(t);
+      if (b == kNone) {
+        unlock(idx, t);
+        return false;
+      }
+      node_regs<W> left, right;
+      build_from_merged<W>(n, pos, key, val, 0, kSplitLeft, left, t);
+      build_from_merged<W>(n, pos, key, val, kSplitLeft, kDataPairs + 1 - kSplitLeft, right, t);
+      uint32_t rmin = t.shfl(right.k[0], 0);
+      const uint32_t older = versioned ? h.older() : kNone;
+      header hr{kEmptyKey, kNone, ts, (h.level() << 28) | older};
+      header hl{rmin, b, ts, (h.level() << 28) | older};
+      set_header<W>(right, hr, t);
+      set_header<W>(left, hl, t);
+      store<W>(b, right, t);
+      store<W>(a, left, t);
+      __threadfence();
+      // new root content: {0, a}, {rmin, b}
+      node_regs<W> root;
+#pragma unroll
+      for (int j = 0; j < 16 / W; ++j) {
+        int q     = pair_index<W>(t, j);
+        root.k[j] = q == 0 ? 0u : (q == 1 ? rmin : kEmptyKey);
+        root.v[j] = q == 0 ? a : (q == 1 ? b : kEmptyKey);
+      }
+      header hroot{kEmptyKey, kNone | kLockBit, versioned ? E : h.ts, ((h.level() + 1) << 28) | older};
+      set_header<W>(root, hroot, t);
+      store<W>(idx, root, t);
+      if (t.thread_rank() == 0) atomicAdd(&ctl->stat_split, 1ull);
+      unlock(idx, t);
+      sep_child = kNone;
+      return true;
+    }
+    uint32_t r = alloc(t);
+    if (r == kNone) {
+      unlock(idx, t);
+      return false;
+    }
+    node_regs<W> left, right;
+    build_from_merged<W>(n, pos, key, val, 0, kSplitLeft, left, t);
+    build_from_merged<W>(n, pos, key, val, kSplitLeft, kDataPairs + 1 - kSplitLeft, right, t);
+    uint32_t rmin = t.shfl(right.k[0], 0);
+    header hr{h.high, h.sibling(), ts, (h.level() << 28) | (versioned ? h.older() : kNone)};
+    header hl{rmin, r | kLockBit, h.ts, h.ol};
+    set_header<W>(right, hr, t);
+    set_header<W>(left, hl, t);
+    store<W>(r, right, t);
+    __threadfence();
+    store<W>(idx, left, t);
+    if (t.thread_rank() == 0) atomicAdd(&ctl->stat_split, 1ull);
+    unlock(idx, t);
+    sep_key   = rmin;
+    sep_child = r;
+    return true;
+  }
+
+  // Insert or update key -> value in write epoch E. Returns true on success.
+  template <int W, class Tile>
+  MVBT_DEV bool cooperative_insert(uint32_t key, uint32_t value, const Tile& t, uint32_t E) const {
+    if (key == kEmptyKey) return false;
+    {
+      uint32_t path0 = kNone, path1 = kNone, top = 0;
+      uint32_t leaf = descend_for_write<W>(key, path0, path1, top, t);
+      if (leaf == kNone) return false;
+      node_regs<W> n;
+      header h;
+      leaf = lock_covering<W>(leaf, 0, key, n, h, t);
+      if (leaf == kNone) return false;
+      // update in place if present
+      int pos = find_pos<W>(n, key, t);
+      if (pos >= 0) {
+        if (!prepare_write<W>(leaf, n, h, E, t)) {
+          unlock(leaf, t);
+          return false;
+        }
+#pragma unroll
+        for (int j = 0; j < 16 / W; ++j)
+          if (pair_index<W>(t, j) == pos) n.v[j] = value;
+        store<W>(leaf, n, t);
+        unlock(leaf, t);
+        return true;
+      }
+      if (!prepare_write<W>(leaf, n, h, E, t)) {
+        unlock(leaf, t);
+        return false;
+      }
+      int nvalid = count_valid<W>(n, t);
+      if (nvalid < kDataPairs) {
+        int ipos = count_less<W>(n, key, t);
+        node_regs<W> out;
+        build_from_merged<W>(n, ipos, key, value, 0, nvalid + 1, out, t);
+        store<W>(leaf, out, t);
+        unlock(leaf, t);
+        return true;
+      }
+      // full leaf: split, then push separators up
+      uint32_t sep_key = 0, sep_child = kNone;
+      if (!split_insert<W>(leaf, n, h, key, value, E, sep_key, sep_child, t)) return false;
+      uint32_t level = 1;
+      while (sep_child != kNone) {
+        uint32_t start;
+        if (level <= top) {
+          start = (level < (uint32_t)W) ? t.shfl(path0, level) : t.shfl(path1, level - W);
+          if (start == kNone) start = kRoot;
+        } else {
+          start = kRoot;
+        }
+        if (level >= (uint32_t)kMaxLevels) {
+          if (t.thread_rank() == 0) set_error(kErrCorrupt);
+          return false;
+        }
+        uint32_t p = lock_covering<W>(start, level, sep_key, n, h, t);
+        if (p == kNone) return false;
+        if (!prepare_write<W>(p, n, h, E, t)) {
+          unlock(p, t);
+          return false;
+        }
+        nvalid = count_valid<W>(n, t);
+        if (nvalid < kDataPairs) {
+          int ipos = count_less<W>(n, sep_key, t);
+          node_regs<W> out;
+          build_from_merged<W>(n, ipos, sep_key, sep_child, 0, nvalid + 1, out, t);
+          store<W>(p, out, t);
+          unlock(p, t);
+          return true;
+        }
+        uint32_t k2 = sep_key, c2 = sep_child;
+        if (!split_insert<W>(p, n, h, k2, c2, E, sep_key, sep_child, t)) return false;
+        ++level;
+      }
+      return true;
+    }
+  }
+
+  // Erase key in write epoch E. Returns true if the key was present.
+  template <int W, class Tile>
+  MVBT_DEV bool cooperative_erase(uint32_t key, const Tile& t, uint32_t E) const {
+    if (key == kEmptyKey) return false;
+    uint32_t path0 = kNone, path1 = kNone, top = 0;
+    uint32_t leaf = descend_for_write<W>(key, path0, path1, top, t);
+    if (leaf == kNone) return false;
+    node_regs<W> n;
+    header h;
+    leaf = lock_covering<W>(leaf, 0, key, n, h, t);
+    if (leaf == kNone) return false;
+    int pos = find_pos<W>(n, key, t);
+    if (pos < 0) {
+      unlock(leaf, t);
+      return false;
+    }
+    if (!prepare_write<W>(leaf, n, h, E, t)) {
+      unlock(leaf, t);
+      return false;
+    }
+    remove_at<W>(n, pos, t);
+    store<W>(leaf, n, t);
+    unlock(leaf, t);
+    return true;
+  }
+
+  // Snapshot: returns the id of the new snapshot (the pre-increment epoch).
+  template <class Tile>
+  MVBT_DEV uint32_t take_snapshot(const Tile& t) const {
+    __threadfence();
+    uint32_t s = 0;
+    if (t.thread_rank() == 0) s = atomicAdd(&ctl->epoch, 1u);
+    return t.shfl(s, 0);
+  }
+};
+
+}  // namespace mvbt

@@ -1,0 +1,276 @@
+"""B200-native multiversion B-link tree.
+
+Python mirror of the reference's host API (owensgroup/MVGpuBTree: ``GpuBTree::gpu_blink_tree`` in
+include/gpu_blink_tree.hpp and ``GpuBTree::gpu_versioned_btree`` in
+include/gpu_versioned_blink_tree.hpp) over the C ABI of ``libmvbt.so`` (include/mvbt.h). Method
+names, argument order and meaning follow the reference; arrays are CUDA tensors, pinned host
+tensors or raw device pointers (ints), exactly as the reference's methods take device (or UVA
+pinned) pointers. Every operation runs the library's sm_100a kernels; there is no CPU fallback:
+importing this package fails if the library has not been built.
+"""
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+
+__all__ = [
+    "LATEST", "NOT_FOUND", "MVBTError", "lib", "library_path", "gpu_blink_tree",
+    "gpu_versioned_btree", "gpu_versioned_blink_tree", "pair_dtype_words",
+]
+
+LATEST = 0xFFFFFFFF
+NOT_FOUND = 0xFFFFFFFF
+pair_dtype_words = 2  # a result pair is two uint32 words {key, value}
+
+_HERE = Path(__file__).resolve().parent
+library_path = _HERE / "libmvbt.so"
+
+if not library_path.exists():
+    raise ImportError(
+        f"{library_path} is missing: build it with `python mvgpubtree_b200/build.py` "
+        "(the tree has no CPU implementation)")
+
+lib = ctypes.CDLL(str(library_path))
+
+_u32, _u64, _i32, _vp = ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int32, ctypes.c_void_p
+
+
+class mvbt_config(ctypes.Structure):
+    _fields_ = [("pool_bytes", _u64), ("device", _i32), ("tile_width", _i32),
+                ("block_size", _i32), ("spin_limit", _u32), ("chunk_nodes", _u32),
+                ("reserved", _u32 * 7)]
+
+
+class mvbt_report(ctypes.Structure):
+    _fields_ = [("height", _u32), ("reserved0", _u32), ("keys", _u64), ("leaves", _u64),
+                ("interior", _u64), ("nodes_allocated", _u64), ("key_checksum", _u64),
+                ("locked_nodes", _u32), ("violations", _u32)]
+
+
+class mvbt_device_view(ctypes.Structure):
+    _fields_ = [("pool", _vp), ("control", _vp), ("versioned", _u32), ("capacity", _u32)]
+
+
+def _sig(name, res, *args):
+    f = getattr(lib, name)
+    f.restype = res
+    f.argtypes = list(args)
+    return f
+
+
+_P = _vp
+_sig("mvbt_config_init", None, ctypes.POINTER(mvbt_config))
+_sig("mvbt_create", ctypes.c_int, ctypes.c_int, ctypes.POINTER(mvbt_config), ctypes.POINTER(_vp))
+_sig("mvbt_destroy", ctypes.c_int, _vp)
+_sig("mvbt_insert", ctypes.c_int, _vp, _P, _P, _u32, _vp, ctypes.c_int)
+_sig("mvbt_find", ctypes.c_int, _vp, _P, _P, _u32, _u32, _vp, ctypes.c_int)
+_sig("mvbt_erase", ctypes.c_int, _vp, _P, _u32, _vp, ctypes.c_int)
+_sig("mvbt_range_query", ctypes.c_int, _vp, _P, _P, _P, _P, _u32, _u32, _u32, _vp, ctypes.c_int)
+_sig("mvbt_concurrent_insert_range", ctypes.c_int, _vp, _P, _P, _u32, _P, _P, _u32, _P, _u32, _P, _vp)
+_sig("mvbt_concurrent_find_erase", ctypes.c_int, _vp, _P, _P, _u32, _P, _u32, _vp)
+_sig("mvbt_take_snapshot", ctypes.c_int, _vp, _vp, ctypes.POINTER(_u32))
+_sig("mvbt_take_snapshot_async", ctypes.c_int, _vp, _vp, _P)
+_sig("mvbt_check_errors", ctypes.c_int, _vp, _vp, ctypes.POINTER(_u32))
+_sig("mvbt_clear_errors", ctypes.c_int, _vp, _vp)
+_sig("mvbt_memory_usage", ctypes.c_int, _vp, ctypes.POINTER(_u64), ctypes.POINTER(_u64), ctypes.POINTER(_u64))
+_sig("mvbt_validate", ctypes.c_int, _vp, _u32, ctypes.POINTER(mvbt_report))
+_sig("mvbt_get_device_view", ctypes.c_int, _vp, ctypes.POINTER(mvbt_device_view))
+_sig("mvbt_get_info", ctypes.c_int, _vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+     ctypes.POINTER(ctypes.c_int))
+_sig("mvbt_last_error", ctypes.c_char_p)
+_sig("mvbt_status_string", ctypes.c_char_p, ctypes.c_int)
+
+
+class MVBTError(RuntimeError):
+    """A C ABI call returned a non-zero status."""
+
+    def __init__(self, status: int, where: str):
+        self.status = status
+        msg = lib.mvbt_status_string(status).decode()
+        detail = lib.mvbt_last_error().decode()
+        super().__init__(f"{where}: {msg} ({status}){': ' + detail if detail else ''}")
+
+
+def _check(status: int, where: str) -> None:
+    if status != 0:
+        raise MVBTError(status, where)
+
+
+def _ptr(x, word_bytes: int = 4, name: str = "array"):
+    """Device address of a CUDA tensor, a pinned host tensor or a raw pointer (int)."""
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return x
+    if hasattr(x, "data_ptr"):
+        if x.element_size() not in (4, 8):
+            raise TypeError(f"{name}: expected 32- or 64-bit elements, got {x.element_size()} bytes")
+        if not x.is_contiguous():
+            raise ValueError(f"{name} must be contiguous")
+        if not x.is_cuda and not x.is_pinned():
+            raise ValueError(f"{name} must be a CUDA tensor or pinned host memory; "
+                             "pageable host memory cannot be read by the kernels")
+        return x.data_ptr()
+    raise TypeError(f"{name}: expected a torch tensor or an integer device pointer")
+
+
+def _numel(x) -> int:
+    return int(x.numel()) if hasattr(x, "numel") else 0
+
+
+def _stream(stream) -> int:
+    if stream is None:
+        try:
+            import torch
+            if torch.cuda.is_available() and torch.cuda.is_initialized():
+                return int(torch.cuda.current_stream().cuda_stream)
+        except Exception:
+            pass
+        return 0
+    if isinstance(stream, int):
+        return stream
+    if hasattr(stream, "cuda_stream"):
+        return int(stream.cuda_stream)
+    raise TypeError("stream must be None, an int handle or a torch.cuda.Stream")
+
+
+class _TreeBase:
+    """Shared host methods of both trees (one handle owns one device tree)."""
+
+    _kind = -1
+    branching_factor = 16  # node pairs, as GpuBTree::*::branching_factor
+
+    def __init__(self, pool_bytes: int = 4 << 30, tile_width: int = 8, device: int | None = None,
+                 block_size: int = 256, spin_limit: int = 0, chunk_nodes: int = 0):
+        cfg = mvbt_config()
+        lib.mvbt_config_init(ctypes.byref(cfg))
+        cfg.pool_bytes = int(pool_bytes)
+        cfg.tile_width = int(tile_width)
+        cfg.block_size = int(block_size)
+        cfg.device = -1 if device is None else int(device)
+        cfg.spin_limit = int(spin_limit)
+        cfg.chunk_nodes = int(chunk_nodes)
+        h = _vp()
+        _check(lib.mvbt_create(self._kind, ctypes.byref(cfg), ctypes.byref(h)), "mvbt_create")
+        self._h = h
+        self.tile_width = int(tile_width)
+
+    # -- lifetime --
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib.mvbt_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self) -> int:
+        return int(self._h.value)
+
+    # -- host bulk operations (reference: gpu_blink_tree.hpp:218-265) --
+    def insert(self, keys, values, num_keys: int | None = None, stream=None, in_place: bool = True):
+        n = _numel(keys) if num_keys is None else int(num_keys)
+        _check(lib.mvbt_insert(self._h, _ptr(keys, name="keys"), _ptr(values, name="values"), n,
+                               _stream(stream), int(bool(in_place))), "insert")
+
+    def find(self, keys, values, num_keys: int | None = None, timestamp: int = LATEST, stream=None,
+             concurrent: bool = False):
+        n = _numel(keys) if num_keys is None else int(num_keys)
+        _check(lib.mvbt_find(self._h, _ptr(keys, name="keys"), _ptr(values, name="values"), n,
+                             int(timestamp), _stream(stream), int(bool(concurrent))), "find")
+
+    def erase(self, keys, num_keys: int | None = None, stream=None, concurrent: bool = False):
+        n = _numel(keys) if num_keys is None else int(num_keys)
+        _check(lib.mvbt_erase(self._h, _ptr(keys, name="keys"), n, _stream(stream),
+                              int(bool(concurrent))), "erase")
+
+    def range_query(self, lower_bound, upper_bound, result, counts, average_range_length: int,
+                    num_keys: int | None = None, timestamp: int = LATEST, stream=None,
+                    concurrent: bool = False):
+        n = _numel(lower_bound) if num_keys is None else int(num_keys)
+        _check(lib.mvbt_range_query(self._h, _ptr(lower_bound, name="lower"), _ptr(upper_bound, name="upper"),
+                                    _ptr(result, 8, "result"), _ptr(counts, name="counts"),
+                                    int(average_range_length), n, int(timestamp), _stream(stream),
+                                    int(bool(concurrent))), "range_query")
+
+    def concurrent_insert_range(self, keys, values, num_insertion: int, lower_bound, upper_bound,
+                                num_ranges: int, result, average_range_length: int, counts=None,
+                                stream=None):
+        _check(lib.mvbt_concurrent_insert_range(
+            self._h, _ptr(keys, name="keys"), _ptr(values, name="values"), int(num_insertion),
+            _ptr(lower_bound, name="lower"), _ptr(upper_bound, name="upper"), int(num_ranges),
+            _ptr(result, 8, "result"), int(average_range_length), _ptr(counts, name="counts"),
+            _stream(stream)), "concurrent_insert_range")
+
+    def concurrent_find_erase(self, find_keys, find_results, num_finds: int, erase_keys,
+                              num_erasures: int, stream=None):
+        _check(lib.mvbt_concurrent_find_erase(
+            self._h, _ptr(find_keys, name="find_keys"), _ptr(find_results, name="find_results"),
+            int(num_finds), _ptr(erase_keys, name="erase_keys"), int(num_erasures), _stream(stream)),
+            "concurrent_find_erase")
+
+    # -- status, statistics, validation --
+    def check_errors(self, stream=None, raise_on_error: bool = True) -> int:
+        bits = _u32(0)
+        st = lib.mvbt_check_errors(self._h, _stream(stream), ctypes.byref(bits))
+        if st and raise_on_error:
+            raise MVBTError(st, "device error")
+        return int(bits.value)
+
+    def clear_errors(self, stream=None) -> None:
+        _check(lib.mvbt_clear_errors(self._h, _stream(stream)), "clear_errors")
+
+    def compute_memory_usage(self) -> dict:
+        a, b, c = _u64(), _u64(), _u64()
+        _check(lib.mvbt_memory_usage(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)),
+               "memory_usage")
+        return {"nodes_allocated": a.value, "bytes_allocated": b.value, "pool_bytes": c.value}
+
+    def validate_tree_structure(self, timestamp: int = LATEST, raise_on_error: bool = True) -> dict:
+        rep = mvbt_report()
+        st = lib.mvbt_validate(self._h, int(timestamp), ctypes.byref(rep))
+        out = {f: getattr(rep, f) for f, _ in mvbt_report._fields_ if not f.startswith("reserved")}
+        if st and raise_on_error:
+            raise MVBTError(st, f"validate_tree_structure {out}")
+        return out
+
+    def device_view(self) -> mvbt_device_view:
+        v = mvbt_device_view()
+        _check(lib.mvbt_get_device_view(self._h, ctypes.byref(v)), "device_view")
+        return v
+
+
+class gpu_blink_tree(_TreeBase):
+    """Plain concurrent B-link tree (reference: include/gpu_blink_tree.hpp:63-67)."""
+
+    _kind = 0
+
+
+class gpu_versioned_btree(_TreeBase):
+    """Multiversion B-link tree with snapshots (reference: include/gpu_versioned_blink_tree.hpp:71-75)."""
+
+    _kind = 1
+
+    def take_snapshot(self, stream=None) -> int:
+        """Takes a snapshot and returns its id; synchronises the stream (reference 297-302)."""
+        ts = _u32(0)
+        _check(lib.mvbt_take_snapshot(self._h, _stream(stream), ctypes.byref(ts)), "take_snapshot")
+        return int(ts.value)
+
+    def take_snapshot_async(self, d_out, stream=None) -> None:
+        """Stream-ordered snapshot; writes the id to the device word d_out."""
+        _check(lib.mvbt_take_snapshot_async(self._h, _stream(stream), _ptr(d_out, name="d_out")),
+               "take_snapshot_async")
+
+
+gpu_versioned_blink_tree = gpu_versioned_btree
