@@ -65,7 +65,11 @@ typedef struct mvbt_config {
   int32_t block_size;   /* threads per block of the bulk kernels (0 = 256) */
   uint32_t spin_limit;  /* bounded-wait attempts before an op gives up (0 = 1<<20) */
   uint32_t chunk_nodes; /* nodes per per-SM allocation chunk (0 = 64) */
-  uint32_t reserved[7];
+  uint32_t blocks_per_sm; /* resident blocks per SM of the bulk kernels (0 = full occupancy) */
+  uint32_t max_blocks;  /* hard cap on the grid of the bulk kernels (0 = none) */
+  uint32_t wait_ms;     /* wall-clock limit of one bounded wait, ms (0 = 2000); a lock queue of
+                           every resident tile on one node drains in ~0.1 s */
+  uint32_t reserved[4];
 } mvbt_config;
 
 /* Structural report of a host walk over a copy of the node pool (mvbt_validate). */
@@ -170,8 +174,61 @@ int mvbt_memory_usage(mvbt_tree* tree, uint64_t* nodes_allocated, uint64_t* byte
  * include/gpu_versioned_blink_tree.hpp:1098-1259). */
 int mvbt_validate(mvbt_tree* tree, uint32_t timestamp, mvbt_report* report);
 
+/* The same walk over a HOST image of the pool (nodes * 32 words, node i at word 32 * i), e.g. a
+ * dump taken with cudaMemcpy; versioned selects snapshot resolution. Needs no GPU. */
+int mvbt_validate_image(const uint32_t* image, uint64_t nodes, int versioned, uint32_t timestamp,
+                        mvbt_report* report);
+
+/* As mvbt_validate_image, and writes a text description of the first violations (NUL-terminated,
+ * at most detail_len bytes) into the HOST buffer detail. */
+int mvbt_validate_image_detail(const uint32_t* image, uint64_t nodes, int versioned,
+                               uint32_t timestamp, mvbt_report* report, char* detail,
+                               uint64_t detail_len);
+
+/* Copies up to max_nodes allocated nodes (node i = 32 words) into the HOST buffer dst and
+ * returns the number copied in *nodes; synchronises the device. The image can be checked with
+ * mvbt_validate_image or stored as a dump of the tree. */
+int mvbt_copy_pool(mvbt_tree* tree, void* dst, uint64_t max_nodes, uint64_t* nodes);
+
 /* Device view for user kernels calling the cooperative_* device API. */
 int mvbt_get_device_view(mvbt_tree* tree, mvbt_device_view* out);
+
+/* ---------------------------------------------------------------------------------------------
+ * Mixed operation batches (versioned trees). Batch b holds ops [batch_off[b], batch_off[b+1]);
+ * op i is type[i] (MVBT_OP_*), key[i] and arg[i] (the value of an insert, the exclusive upper
+ * bound of a range query). One snapshot per batch: batch b reads at the snapshot taken when it
+ * starts and writes after it, so every result equals that of the batches applied one by one, in
+ * order. result[i] receives a find's value (or MVBT_NOT_FOUND) or a range query's full count (0
+ * for writes); range query i writes at most range_cap[i] pairs at range_out + out_off[i].
+ * Writes inside one batch must touch distinct keys. No counterpart exists in the reference,
+ * whose callers issue each op kind of a batch as its own launch
+ * (include/gpu_versioned_blink_tree.hpp:106-216); MVBT_BATCH_PER_LAUNCH is that plain method
+ * (one snapshot + one launch per batch).
+ * ------------------------------------------------------------------------------------------- */
+#define MVBT_OP_FIND 0u
+#define MVBT_OP_INSERT 1u
+#define MVBT_OP_ERASE 2u
+#define MVBT_OP_RANGE 3u
+
+#define MVBT_BATCH_PERSISTENT 0 /* one persistent launch fed by a device work queue */
+#define MVBT_BATCH_PER_LAUNCH 1 /* one snapshot and one launch per batch */
+#define MVBT_BATCH_GRAPH 2      /* the persistent launch captured once and replayed as a CUDA graph */
+
+typedef struct mvbt_batch_plan mvbt_batch_plan;
+
+/* Allocates the device scratch of the batched path for up to max_ops ops in max_batches batches. */
+int mvbt_batch_plan_create(mvbt_tree* tree, uint64_t max_ops, uint32_t max_batches,
+                           mvbt_batch_plan** out);
+int mvbt_batch_plan_destroy(mvbt_batch_plan* plan);
+
+/* Runs num_batches batches. batch_off is a HOST array of num_batches + 1 offsets; the op arrays
+ * are device arrays. Stream ordered; the call waits for the plan's previous run on `stream`
+ * before it reuses the plan's staging memory. MVBT_BATCH_GRAPH re-captures when an array
+ * pointer or the stream changes. */
+int mvbt_batch_run(mvbt_batch_plan* plan, uint32_t num_batches, const uint64_t* batch_off,
+                   const uint32_t* type, const uint32_t* key, const uint32_t* arg,
+                   const uint64_t* out_off, const uint32_t* range_cap, uint32_t* result,
+                   mvbt_pair* range_out, int mode, void* stream);
 
 /* Tree kind, tile width and device of a handle. */
 int mvbt_get_info(mvbt_tree* tree, int* kind, int* tile_width, int* device);

@@ -44,15 +44,49 @@
 //     control block and returns (no trap, no unbounded loop).
 #pragma once
 
-#include <cooperative_groups.h>
 #include <cstdint>
 
+#if defined(MVBT_HOST_EMULATION)
+// Host build of this header for the CPU emulation harness (tests/emu): each W-lane tile runs as W
+// host threads and the CUDA primitives below map to GCC atomics. The sm_100a build never sees
+// this branch.
+#include <atomic>
+#include <chrono>
+#include <thread>
+#define MVBT_DEV inline
+struct uint2 {
+  uint32_t x, y;
+};
+inline uint2 make_uint2(uint32_t x, uint32_t y) { return uint2{x, y}; }
+inline int __popc(uint32_t x) { return __builtin_popcount(x); }
+inline int __ffs(uint32_t x) { return __builtin_ffs((int)x); }
+inline int __clz(uint32_t x) { return x ? __builtin_clz(x) : 32; }
+inline void __threadfence() { std::atomic_thread_fence(std::memory_order_seq_cst); }
+inline void __nanosleep(unsigned) { std::this_thread::yield(); }
+template <class T, class U>
+inline T atomicOr(T* p, U v) { return __atomic_fetch_or(p, (T)v, __ATOMIC_SEQ_CST); }
+template <class T, class U>
+inline T atomicAnd(T* p, U v) { return __atomic_fetch_and(p, (T)v, __ATOMIC_SEQ_CST); }
+template <class T, class U>
+inline T atomicAdd(T* p, U v) { return __atomic_fetch_add(p, (T)v, __ATOMIC_SEQ_CST); }
+template <class T, class U>
+inline T atomicExch(T* p, U v) { return __atomic_exchange_n(p, (T)v, __ATOMIC_SEQ_CST); }
+namespace mvbt {
+namespace emu {
+inline thread_local uint32_t sm = 0;  // emulated SM id of the calling lane
+}
+}  // namespace mvbt
+#else
+#include <cooperative_groups.h>
 #ifndef MVBT_DEV
 #define MVBT_DEV __device__ __forceinline__
 #endif
+#endif
 
 namespace mvbt {
+#if !defined(MVBT_HOST_EMULATION)
 namespace cg = cooperative_groups;
+#endif
 
 // ----------------------------------------------------------------------------------------------
 // Constants
@@ -96,6 +130,41 @@ struct control_block {
   unsigned long long sm_pool[kMaxSmSlots];  // per-SM chunk cursor: (base << 32) | used
 };
 
+#if defined(MVBT_HOST_EMULATION)
+#define MVBT_HD inline
+#else
+#define MVBT_HD __host__ __device__ __forceinline__
+#endif
+
+// Word t (0..31) of the initial root: a leaf holding the tombstone {0, 0}, empty pairs,
+// high key 0xFFFFFFFF, no sibling, ts 0, no older version, level 0.
+MVBT_HD uint32_t initial_root_word(int t) {
+  if (t == 0 || t == 1) return 0u;
+  if (t < 28) return kEmptyKey;
+  if (t == 28) return kEmptyKey;  // high key
+  if (t == 29) return kNone;      // link
+  if (t == 30) return 0u;         // ts
+  return kNone;                   // older | level 0
+}
+
+MVBT_HD void init_control(control_block& c, uint32_t capacity, uint32_t chunk, uint32_t spin_limit,
+                          uint32_t wait_ns) {
+  c.epoch         = 0;
+  c.error         = 0;
+  c.bump          = 1;  // node 0 is the root
+  c.capacity      = capacity;
+  c.chunk         = chunk;
+  c.spin_limit    = spin_limit;
+  c.wait_ns       = wait_ns;
+  c.reserved      = 0;
+  c.stat_cow      = 0;
+  c.stat_split    = 0;
+  c.stat_restart  = 0;
+  c.stat_reserved = 0;
+  // used == chunk: the first allocation on each SM refills its chunk from the bump pointer
+  for (int i = 0; i < kMaxSmSlots; ++i) c.sm_pool[i] = chunk;
+}
+
 // ----------------------------------------------------------------------------------------------
 // Low-level memory access
 // ----------------------------------------------------------------------------------------------
@@ -106,6 +175,32 @@ struct node_regs {
   uint32_t v[P];
 };
 
+#if defined(MVBT_HOST_EMULATION)
+MVBT_DEV uint32_t sm_id() { return emu::sm; }
+MVBT_DEV unsigned long long global_ns() {
+  return (unsigned long long)std::chrono::duration_cast<std::chrono::nanoseconds>(
+             std::chrono::steady_clock::now().time_since_epoch())
+      .count();
+}
+MVBT_DEV uint32_t ld_relaxed_u32(const uint32_t* p) { return __atomic_load_n(p, __ATOMIC_RELAXED); }
+MVBT_DEV unsigned long long ld_relaxed_u64(const unsigned long long* p) {
+  return __atomic_load_n(p, __ATOMIC_RELAXED);
+}
+template <int W>
+MVBT_DEV void ld_lane(const uint32_t* p, node_regs<W>& n, bool) {
+  for (int j = 0; j < 16 / W; ++j) {
+    n.k[j] = __atomic_load_n(p + 2 * j, __ATOMIC_RELAXED);
+    n.v[j] = __atomic_load_n(p + 2 * j + 1, __ATOMIC_RELAXED);
+  }
+}
+template <int W>
+MVBT_DEV void st_lane(uint32_t* p, const node_regs<W>& n) {
+  for (int j = 0; j < 16 / W; ++j) {
+    __atomic_store_n(p + 2 * j, n.k[j], __ATOMIC_RELAXED);
+    __atomic_store_n(p + 2 * j + 1, n.v[j], __ATOMIC_RELAXED);
+  }
+}
+#else
 MVBT_DEV uint32_t sm_id() {
   uint32_t r;
   asm volatile("mov.u32 %0, %%smid;" : "=r"(r));
@@ -170,6 +265,8 @@ MVBT_DEV void st_lane(uint32_t* p, const node_regs<W>& n) {
                  : "memory");
   }
 }
+
+#endif  // MVBT_HOST_EMULATION
 
 // ----------------------------------------------------------------------------------------------
 // Register-resident node helpers (all are tile-collective: every lane must call them)
@@ -519,10 +616,11 @@ struct device_tree {
     return true;
   }
 
-  // Moves from node idx to the version visible at ts (snapshot readers only).
+  // Moves from node idx to the version visible at ts (snapshot readers only). Sets `copy` when it
+  // followed at least one older pointer: such a version is never written again.
   template <int W, class Tile>
   MVBT_DEV bool to_version(uint32_t& idx, node_regs<W>& n, header& h, uint32_t ts, bool strong,
-                           const Tile& t) const {
+                           bool& copy, const Tile& t) const {
     uint32_t hops = 0;
     while (h.ts > ts) {
       uint32_t older = h.older();
@@ -533,9 +631,26 @@ struct device_tree {
       idx = older;
       if (!valid(idx, t)) return false;
       load<W>(idx, n, strong, t);
-      h = get_header<W>(n, t);
+      h    = get_header<W>(n, t);
+      copy = true;
     }
     return true;
+  }
+
+  // A concurrent snapshot reader that is about to use the data of a leaf version it read with
+  // ts <= snapshot re-reads the header after a fence. A writer publishes {ts = E, older = copy}
+  // before it changes the data, so if any lane saw changed data the re-read shows ts > snapshot:
+  // the reader then returns the index of the immutable copy (else kNone: the data is consistent).
+  template <class Tile>
+  MVBT_DEV uint32_t recheck_version(uint32_t idx, uint32_t ts, const Tile& t) const {
+    __threadfence();
+    t.sync();
+    unsigned long long v = 0;
+    if (t.thread_rank() == 0)
+      v = ld_relaxed_u64(reinterpret_cast<const unsigned long long*>(node_ptr(idx) + 30));
+    v            = t.shfl(v, 0);
+    uint32_t ts2 = (uint32_t)v, ol2 = (uint32_t)(v >> 32);
+    return ts2 > ts ? (ol2 & kIndexMask) : kNone;
   }
 
   // ------------------------------------------------------------------------------------------
@@ -546,17 +661,30 @@ struct device_tree {
                                      bool concurrent = false) const {
     const bool snap = versioned && ts != kLatest;
     uint32_t idx    = kRoot;
+    bool via_older  = false;  // idx was reached through an older-version pointer
     node_regs<W> n;
     for (uint32_t step = 0; step < kMaxSteps; ++step) {
       if (!valid(idx, t)) return kNotFound;
       load<W>(idx, n, concurrent, t);
-      header h = get_header<W>(n, t);
-      if (snap && !to_version<W>(idx, n, h, ts, concurrent, t)) return kNotFound;
+      header h  = get_header<W>(n, t);
+      bool copy = via_older;
+      via_older = false;
+      if (snap && !to_version<W>(idx, n, h, ts, concurrent, copy, t)) return kNotFound;
       if (key >= h.high && h.sibling() != kNone) {
         idx = h.sibling();
         continue;
       }
-      if (h.is_leaf()) return leaf_value<W>(n, key, t);
+      if (h.is_leaf()) {
+        if (snap && concurrent && !copy) {
+          uint32_t older = recheck_version(idx, ts, t);
+          if (older != kNone) {  // changed under us: use the immutable copy instead
+            idx       = older;
+            via_older = true;
+            continue;
+          }
+        }
+        return leaf_value<W>(n, key, t);
+      }
       idx = child_for<W>(n, key, t);
     }
     if (t.thread_rank() == 0) set_error(kErrStepLimit);
@@ -574,24 +702,36 @@ struct device_tree {
     if (hi <= lo) return 0;
     const bool snap = versioned && ts != kLatest;
     uint32_t idx    = kRoot;
+    bool via_older  = false;
     node_regs<W> n;
     header h;
-    uint32_t step = 0;
-    // descend to the leaf that holds lo
-    for (;; ++step) {
+    // descend to the leaf that holds lo and settle on a consistent version of it
+    for (uint32_t step = 0;; ++step) {
       if (step >= kMaxSteps) {
         if (t.thread_rank() == 0) set_error(kErrStepLimit);
         return 0;
       }
       if (!valid(idx, t)) return 0;
       load<W>(idx, n, concurrent, t);
-      h = get_header<W>(n, t);
-      if (snap && !to_version<W>(idx, n, h, ts, concurrent, t)) return 0;
+      h         = get_header<W>(n, t);
+      bool copy = via_older;
+      via_older = false;
+      if (snap && !to_version<W>(idx, n, h, ts, concurrent, copy, t)) return 0;
       if (lo >= h.high && h.sibling() != kNone) {
         idx = h.sibling();
         continue;
       }
-      if (h.is_leaf()) break;
+      if (h.is_leaf()) {
+        if (snap && concurrent && !copy) {
+          uint32_t older = recheck_version(idx, ts, t);
+          if (older != kNone) {
+            idx       = older;
+            via_older = true;
+            continue;
+          }
+        }
+        break;
+      }
       idx = child_for<W>(n, lo, t);
     }
     // scan leaves to the right (a sibling chain is never longer than the pool)
@@ -625,11 +765,30 @@ struct device_tree {
         if (t.thread_rank() == 0) set_error(kErrStepLimit);
         break;
       }
-      idx = h.sibling();
-      if (!valid(idx, t)) break;
-      load<W>(idx, n, concurrent, t);
-      h = get_header<W>(n, t);
-      if (snap && !to_version<W>(idx, n, h, ts, concurrent, t)) break;
+      // next leaf: load, resolve the snapshot version, validate before its data is used
+      idx           = h.sibling();
+      bool settled  = false;
+      for (uint32_t tries = 0; tries < kMaxSteps && !settled; ++tries) {
+        if (!valid(idx, t)) return count;
+        load<W>(idx, n, concurrent, t);
+        h         = get_header<W>(n, t);
+        bool copy = via_older;
+        via_older = false;
+        if (snap && !to_version<W>(idx, n, h, ts, concurrent, copy, t)) return count;
+        if (snap && concurrent && !copy) {
+          uint32_t older = recheck_version(idx, ts, t);
+          if (older != kNone) {
+            idx       = older;
+            via_older = true;
+            continue;
+          }
+        }
+        settled = true;
+      }
+      if (!settled) {
+        if (t.thread_rank() == 0) set_error(kErrStepLimit);
+        return count;
+      }
     }
     return count;
   }
@@ -907,5 +1066,131 @@ struct device_tree {
     return t.shfl(s, 0);
   }
 };
+
+// ----------------------------------------------------------------------------------------------
+// Mixed operation batches
+//
+// A batch is a list of ops {type, key, arg}: find (arg unused), insert (arg = value), erase, and
+// range query (arg = exclusive upper bound, output slot at range_out + out_off[i] holding at most
+// cap[i] pairs). One snapshot per batch: batch b reads at snapshot S0 + b and writes in epoch
+// S0 + b + 1, so every result is that of the batch applied after all earlier batches. The
+// reference issues each op kind of a batch as its own host launch
+// (include/gpu_versioned_blink_tree.hpp:106-216); here a batch is one launch, or many batches
+// are one persistent launch.
+// ----------------------------------------------------------------------------------------------
+enum : uint32_t { kOpFind = 0, kOpInsert = 1, kOpErase = 2, kOpRange = 3 };
+
+struct batch_view {
+  const uint32_t* type;
+  const uint32_t* key;
+  const uint32_t* arg;
+  const uint64_t* out_off;  // range output offset, pairs
+  const uint32_t* cap;      // range output capacity, pairs
+  uint32_t* result;         // find value or range count (0 for writes)
+  uint2* range_out;
+};
+
+MVBT_DEV bool is_write_op(uint32_t type) { return type == kOpInsert || type == kOpErase; }
+
+// Runs op i of a batch; returns true if it was a write.
+template <int W, class Tile>
+MVBT_DEV bool run_batch_op(const device_tree& T, const batch_view& B, uint64_t i, uint32_t S,
+                           uint32_t E, const Tile& t) {
+  const uint32_t ty = B.type[i], k = B.key[i];
+  uint32_t r        = 0;
+  bool write        = false;
+  if (ty == kOpFind) {
+    r = T.cooperative_find<W>(k, t, S, true);
+  } else if (ty == kOpRange) {
+    uint2* out = B.range_out ? B.range_out + B.out_off[i] : nullptr;
+    r          = T.cooperative_range_query<W>(k, B.arg[i], t, S, out, B.cap[i], true);
+  } else if (ty == kOpInsert) {
+    T.cooperative_insert<W>(k, B.arg[i], t, E);
+    write = true;
+  } else if (ty == kOpErase) {
+    T.cooperative_erase<W>(k, t, E);
+    write = true;
+  }
+  if (t.thread_rank() == 0) B.result[i] = r;
+  return write;
+}
+
+// Schedule of the persistent batched launch: claim positions run batch by batch, writes first
+// inside each batch (perm maps a claim position to an op index), and a batch may start only
+// once every write of the previous batch has finished.
+struct batch_sched {
+  const uint64_t* batch_off;  // [num_batches + 1] claim positions of each batch
+  const uint32_t* perm;       // claim position -> op index
+  const uint32_t* n_writes;   // [num_batches] writes per batch
+  uint32_t* writes_done;      // [num_batches] finished writes (zero at launch)
+  unsigned long long* cursor; // next unclaimed position (zero at launch)
+  const uint32_t* params;     // device words: [0] num_batches, [1] snapshot of batch 0
+  uint32_t chunk;             // positions claimed per tile at a time
+};
+
+// Worker loop of one tile in the persistent batched launch.
+template <int W, class Tile>
+MVBT_DEV void batched_worker(const device_tree& T, const batch_view& B, const batch_sched& sc,
+                             const Tile& t) {
+  const uint32_t nb    = ld_relaxed_u32(sc.params + 0);
+  const uint32_t S0    = ld_relaxed_u32(sc.params + 1);
+  const uint64_t total = sc.batch_off[nb];
+  uint32_t b           = 0;   // batch of the current position (positions only grow)
+  uint32_t ready       = 0;   // every batch < ready may run
+  uint32_t pending     = 0;   // finished writes of batch b not yet published
+  const unsigned long long lns = T.ctl->wait_ns;
+  for (;;) {
+    unsigned long long base = 0;
+    if (t.thread_rank() == 0) base = atomicAdd(sc.cursor, (unsigned long long)sc.chunk);
+    base = t.shfl(base, 0);
+    if (base >= total) break;
+    const uint64_t end = base + sc.chunk < total ? base + sc.chunk : total;
+    for (uint64_t p = base; p < end; ++p) {
+      while (p >= sc.batch_off[b + 1]) {
+        if (pending && t.thread_rank() == 0) atomicAdd(&sc.writes_done[b], pending);
+        pending = 0;
+        ++b;
+      }
+      if (b >= ready) {
+        // publish own finished writes first, then wait for the previous batch's writes
+        if (pending) {
+          __threadfence();
+          if (t.thread_rank() == 0) atomicAdd(&sc.writes_done[b], pending);
+          pending = 0;
+        }
+        if (b > 0) {
+          const unsigned long long t0 = global_ns();
+          bool ok = false;
+          for (uint32_t w = 0;; ++w) {
+            uint32_t done = 0;
+            if (t.thread_rank() == 0) done = ld_relaxed_u32(&sc.writes_done[b - 1]);
+            done = t.shfl(done, 0);
+            if (done >= sc.n_writes[b - 1]) {
+              ok = true;
+              break;
+            }
+            if (global_ns() - t0 > lns) break;
+            __nanosleep(w < 16 ? 64 : 256);
+          }
+          if (!ok) {
+            if (t.thread_rank() == 0) T.set_error(kErrSpinLimit);
+          }
+          __threadfence();
+        }
+        ready = b + 1;
+      }
+      const uint32_t i = sc.perm[p];
+      if (run_batch_op<W>(T, B, i, S0 + b, S0 + b + 1, t)) {
+        __threadfence();
+        ++pending;
+      }
+    }
+    if (pending) {
+      __threadfence();
+      if (t.thread_rank() == 0) atomicAdd(&sc.writes_done[b], pending);
+      pending = 0;
+    }
+  }
+}
 
 }  // namespace mvbt

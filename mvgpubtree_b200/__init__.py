@@ -15,7 +15,8 @@ from pathlib import Path
 
 __all__ = [
     "LATEST", "NOT_FOUND", "MVBTError", "lib", "library_path", "gpu_blink_tree",
-    "gpu_versioned_btree", "gpu_versioned_blink_tree", "pair_dtype_words",
+    "gpu_versioned_btree", "gpu_versioned_blink_tree", "pair_dtype_words", "BatchPlan",
+    "BATCH_PERSISTENT", "BATCH_PER_LAUNCH", "BATCH_GRAPH",
 ]
 
 LATEST = 0xFFFFFFFF
@@ -38,7 +39,8 @@ _u32, _u64, _i32, _vp = ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int32, ctypes
 class mvbt_config(ctypes.Structure):
     _fields_ = [("pool_bytes", _u64), ("device", _i32), ("tile_width", _i32),
                 ("block_size", _i32), ("spin_limit", _u32), ("chunk_nodes", _u32),
-                ("reserved", _u32 * 7)]
+                ("blocks_per_sm", _u32), ("max_blocks", _u32), ("wait_ms", _u32),
+                ("reserved", _u32 * 4)]
 
 
 class mvbt_report(ctypes.Structure):
@@ -75,8 +77,15 @@ _sig("mvbt_clear_errors", ctypes.c_int, _vp, _vp)
 _sig("mvbt_memory_usage", ctypes.c_int, _vp, ctypes.POINTER(_u64), ctypes.POINTER(_u64), ctypes.POINTER(_u64))
 _sig("mvbt_validate", ctypes.c_int, _vp, _u32, ctypes.POINTER(mvbt_report))
 _sig("mvbt_get_device_view", ctypes.c_int, _vp, ctypes.POINTER(mvbt_device_view))
+_sig("mvbt_copy_pool", ctypes.c_int, _vp, _vp, _u64, ctypes.POINTER(_u64))
+_sig("mvbt_validate_image", ctypes.c_int, _vp, _u64, ctypes.c_int, _u32, ctypes.POINTER(mvbt_report))
+_sig("mvbt_validate_image_detail", ctypes.c_int, _vp, _u64, ctypes.c_int, _u32, ctypes.POINTER(mvbt_report),
+     ctypes.c_char_p, _u64)
 _sig("mvbt_get_info", ctypes.c_int, _vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
      ctypes.POINTER(ctypes.c_int))
+_sig("mvbt_batch_plan_create", ctypes.c_int, _vp, _u64, _u32, ctypes.POINTER(_vp))
+_sig("mvbt_batch_plan_destroy", ctypes.c_int, _vp)
+_sig("mvbt_batch_run", ctypes.c_int, _vp, _u32, _vp, _P, _P, _P, _P, _P, _P, _P, ctypes.c_int, _vp)
 _sig("mvbt_last_error", ctypes.c_char_p)
 _sig("mvbt_status_string", ctypes.c_char_p, ctypes.c_int)
 
@@ -141,7 +150,8 @@ class _TreeBase:
     branching_factor = 16  # node pairs, as GpuBTree::*::branching_factor
 
     def __init__(self, pool_bytes: int = 4 << 30, tile_width: int = 8, device: int | None = None,
-                 block_size: int = 256, spin_limit: int = 0, chunk_nodes: int = 0):
+                 block_size: int = 256, spin_limit: int = 0, chunk_nodes: int = 0,
+                 blocks_per_sm: int = 0, max_blocks: int = 0, wait_ms: int = 0):
         cfg = mvbt_config()
         lib.mvbt_config_init(ctypes.byref(cfg))
         cfg.pool_bytes = int(pool_bytes)
@@ -150,6 +160,10 @@ class _TreeBase:
         cfg.device = -1 if device is None else int(device)
         cfg.spin_limit = int(spin_limit)
         cfg.chunk_nodes = int(chunk_nodes)
+        cfg.blocks_per_sm = int(blocks_per_sm)
+        cfg.max_blocks = int(max_blocks)
+        if wait_ms:
+            cfg.wait_ms = int(wait_ms)
         h = _vp()
         _check(lib.mvbt_create(self._kind, ctypes.byref(cfg), ctypes.byref(h)), "mvbt_create")
         self._h = h
@@ -244,6 +258,25 @@ class _TreeBase:
             raise MVBTError(st, f"validate_tree_structure {out}")
         return out
 
+    def validate_detail(self, timestamp: int = LATEST) -> tuple[dict, str]:
+        """Host walk of a pool copy; returns the report and a description of the first violations."""
+        img = self.copy_pool()
+        rep = mvbt_report()
+        buf = ctypes.create_string_buffer(8192)
+        lib.mvbt_validate_image_detail(img.ctypes.data, img.shape[0], int(self._kind == 1),
+                                       int(timestamp), ctypes.byref(rep), buf, 8192)
+        out = {f: getattr(rep, f) for f, _ in mvbt_report._fields_ if not f.startswith("reserved")}
+        return out, buf.value.decode()
+
+    def copy_pool(self):
+        """Host image of the allocated nodes: numpy uint32 array [nodes, 32]."""
+        import numpy as np
+        usage = self.compute_memory_usage()
+        img = np.empty((int(usage["nodes_allocated"]), 32), np.uint32)
+        n = _u64(0)
+        _check(lib.mvbt_copy_pool(self._h, img.ctypes.data, img.shape[0], ctypes.byref(n)), "copy_pool")
+        return img[: n.value]
+
     def device_view(self) -> mvbt_device_view:
         v = mvbt_device_view()
         _check(lib.mvbt_get_device_view(self._h, ctypes.byref(v)), "device_view")
@@ -267,10 +300,56 @@ class gpu_versioned_btree(_TreeBase):
         _check(lib.mvbt_take_snapshot(self._h, _stream(stream), ctypes.byref(ts)), "take_snapshot")
         return int(ts.value)
 
+    def batch_plan(self, max_ops: int, max_batches: int) -> "BatchPlan":
+        """Scratch for mixed op batches of up to max_ops ops in max_batches batches."""
+        return BatchPlan(self, max_ops, max_batches)
+
     def take_snapshot_async(self, d_out, stream=None) -> None:
         """Stream-ordered snapshot; writes the id to the device word d_out."""
         _check(lib.mvbt_take_snapshot_async(self._h, _stream(stream), _ptr(d_out, name="d_out")),
                "take_snapshot_async")
+
+
+BATCH_PERSISTENT, BATCH_PER_LAUNCH, BATCH_GRAPH = 0, 1, 2
+
+
+class BatchPlan:
+    """Device scratch and launch plan for running many mixed op batches on a versioned tree.
+
+    run() takes the batch offsets as a host array (numpy uint64, num_batches + 1 entries) and the
+    op arrays as device tensors: type/key/arg (uint32 words), out_off (64-bit), range_cap,
+    result and range_out (pairs). mode: BATCH_PERSISTENT (one persistent launch fed by a device
+    work queue), BATCH_GRAPH (that launch captured once and replayed as a CUDA graph) or
+    BATCH_PER_LAUNCH (the plain method: one snapshot and one launch per batch).
+    """
+
+    def __init__(self, tree: "gpu_versioned_btree", max_ops: int, max_batches: int):
+        h = _vp()
+        _check(lib.mvbt_batch_plan_create(tree._h, int(max_ops), int(max_batches), ctypes.byref(h)),
+               "batch_plan_create")
+        self._h = h
+        self.tree = tree  # keeps the tree alive while the plan exists
+
+    def run(self, batch_off, type, key, arg, out_off, range_cap, result, range_out,
+            mode: int = BATCH_PERSISTENT, stream=None):
+        import numpy as np
+        off = np.ascontiguousarray(batch_off, dtype=np.uint64)
+        _check(lib.mvbt_batch_run(self._h, len(off) - 1, off.ctypes.data, _ptr(type, name="type"),
+                                  _ptr(key, name="key"), _ptr(arg, name="arg"),
+                                  _ptr(out_off, 8, "out_off"), _ptr(range_cap, name="range_cap"),
+                                  _ptr(result, name="result"), _ptr(range_out, 8, "range_out"),
+                                  int(mode), _stream(stream)), "batch_run")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.mvbt_batch_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 gpu_versioned_blink_tree = gpu_versioned_btree

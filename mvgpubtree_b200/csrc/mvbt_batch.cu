@@ -1,0 +1,342 @@
+// Mixed operation batches: one persistent launch for many batches (device work queue, optional
+// CUDA-graph replay) and the plain mode with one host launch per batch.
+//
+// A batch plan owns the scratch the persistent path needs: the claim order (writes first in each
+// batch), per-batch write counters, the claim cursor and a pinned staging area for the batch
+// offsets, so a captured graph can be replayed for any batch list up to the plan's limits.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <string>
+
+#include "mvbt.h"
+#include "mvbt_device.cuh"
+
+namespace cg = cooperative_groups;
+using mvbt::batch_sched;
+using mvbt::batch_view;
+using mvbt::device_tree;
+
+// Internal helpers shared with mvbt_tree.cu.
+extern "C" int mvbt_internal_view(mvbt_tree* t, device_tree* view, int* tile_width, int* block_size,
+                                  int* num_sms, uint32_t* blocks_per_sm, uint32_t* max_blocks,
+                                  void** control);
+extern "C" void mvbt_internal_set_error(const char* msg);
+
+struct mvbt_batch_plan {
+  mvbt_tree* tree;
+  uint64_t max_ops;
+  uint32_t max_batches;
+  // device scratch
+  uint64_t* d_batch_off;  // [max_batches + 1]
+  uint32_t* d_params;     // [0] num_batches, [1] snapshot of batch 0
+  uint32_t* d_perm;       // [max_ops]
+  uint32_t* d_counts;     // n_writes | writes_done | write fill | read fill, each [max_batches]
+  unsigned long long* d_cursor;
+  // pinned staging
+  uint64_t* h_batch_off;
+  uint32_t* h_params;
+  // graph cache
+  cudaGraphExec_t graph;
+  bool have_graph;
+  const void* graph_key[8];
+};
+
+namespace {
+
+constexpr int kPrepassBlocks = 512;
+constexpr int kPrepassThreads = 256;
+
+int fail(int code, const std::string& msg) {
+  mvbt_internal_set_error(msg.c_str());
+  return code;
+}
+
+#define MVBT_TRY(expr)                                                                          \
+  do {                                                                                          \
+    cudaError_t e_ = (expr);                                                                    \
+    if (e_ != cudaSuccess) return fail(MVBT_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+__device__ __forceinline__ uint32_t batch_of(const uint64_t* off, uint32_t nb, uint64_t i) {
+  uint32_t lo = 0, hi = nb;  // largest b with off[b] <= i
+  while (hi - lo > 1) {
+    uint32_t mid = (lo + hi) >> 1;
+    if (__ldg(off + mid) <= i) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// Pass 1: writes per batch (warp-aggregated atomics).
+__global__ void k_count_writes(const uint32_t* __restrict__ type, const uint64_t* __restrict__ off,
+                               const uint32_t* __restrict__ params, uint32_t* n_writes) {
+  const uint32_t nb    = params[0];
+  const uint64_t total = off[nb];
+  const uint32_t lane  = threadIdx.x & 31;
+  const uint64_t warps = (uint64_t)gridDim.x * blockDim.x / 32;
+  for (uint64_t base = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x - lane); base < total;
+       base += warps * 32) {
+    const uint64_t i   = base + lane;
+    const bool w       = i < total && mvbt::is_write_op(type[i]);
+    const uint32_t act = __ballot_sync(0xFFFFFFFFu, w);
+    if (w) {
+      const uint32_t b   = batch_of(off, nb, i);
+      const uint32_t grp = __match_any_sync(act, b);
+      if (lane == (uint32_t)(__ffs(grp) - 1)) atomicAdd(&n_writes[b], (uint32_t)__popc(grp));
+    }
+  }
+}
+
+// Pass 2: claim order with the writes of every batch first.
+__global__ void k_place(const uint32_t* __restrict__ type, const uint64_t* __restrict__ off,
+                        const uint32_t* __restrict__ params, const uint32_t* __restrict__ n_writes,
+                        uint32_t* wfill, uint32_t* rfill, uint32_t* perm) {
+  const uint32_t nb    = params[0];
+  const uint64_t total = off[nb];
+  const uint32_t lane  = threadIdx.x & 31;
+  const uint64_t warps = (uint64_t)gridDim.x * blockDim.x / 32;
+  for (uint64_t base = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x - lane); base < total;
+       base += warps * 32) {
+    const uint64_t i    = base + lane;
+    const bool live     = i < total;
+    const uint32_t livm = __ballot_sync(0xFFFFFFFFu, live);
+    if (!live) continue;
+    const bool w        = mvbt::is_write_op(type[i]);
+    const uint32_t b    = batch_of(off, nb, i);
+    const uint32_t key  = (b << 1) | (w ? 1u : 0u);
+    const uint32_t grp  = __match_any_sync(livm, key);
+    const uint32_t lead = (uint32_t)(__ffs(grp) - 1);
+    const uint32_t rank = __popc(grp & ((1u << lane) - 1u));
+    uint32_t slot       = 0;
+    if (lane == lead) slot = atomicAdd(w ? &wfill[b] : &rfill[b], (uint32_t)__popc(grp));
+    slot = __shfl_sync(grp, slot, lead);
+    const uint64_t pos = off[b] + (w ? 0u : n_writes[b]) + slot + rank;
+    perm[pos]          = (uint32_t)i;
+  }
+}
+
+__global__ void k_batch_begin(mvbt::control_block* ctl, uint32_t* params) {
+  if (threadIdx.x == 0) {
+    __threadfence();
+    params[1] = mvbt::ld_relaxed_u32(&ctl->epoch);
+  }
+}
+
+__global__ void k_batch_end(mvbt::control_block* ctl, const uint32_t* params) {
+  if (threadIdx.x == 0) {
+    __threadfence();
+    atomicExch(&ctl->epoch, params[1] + params[0]);
+  }
+}
+
+template <int W>
+__global__ void __launch_bounds__(256) k_batched(device_tree T, batch_view B, batch_sched sc) {
+  auto tile = cg::tiled_partition<W>(cg::this_thread_block());
+  mvbt::batched_worker<W>(T, B, sc, tile);
+}
+
+// One batch [begin, end) in one launch: reads at the snapshot in snap_word, writes one epoch later.
+template <int W>
+__global__ void __launch_bounds__(256) k_mixed(device_tree T, batch_view B, uint64_t begin,
+                                               uint64_t end, const uint32_t* snap_word) {
+  auto tile        = cg::tiled_partition<W>(cg::this_thread_block());
+  const uint32_t S = mvbt::ld_relaxed_u32(snap_word);
+  const uint64_t tiles = ((uint64_t)gridDim.x * blockDim.x) / W;
+  for (uint64_t i = begin + ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / W; i < end; i += tiles)
+    mvbt::run_batch_op<W>(T, B, i, S, S + 1, tile);
+}
+
+__global__ void k_snapshot_word(mvbt::control_block* ctl, uint32_t* out) {
+  if (threadIdx.x == 0) {
+    __threadfence();
+    *out = atomicAdd(&ctl->epoch, 1u);
+  }
+}
+
+struct launch_ctx {
+  device_tree view;
+  int W, block, sms;
+  uint32_t bps, maxb;
+  mvbt::control_block* ctl;
+};
+
+template <class K>
+unsigned occupancy_grid(const launch_ctx& c, K kernel) {
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, c.block, 0);
+  if (per_sm < 1) per_sm = 1;
+  if (c.bps && (int)c.bps < per_sm) per_sm = (int)c.bps;
+  uint64_t g = (uint64_t)per_sm * c.sms;
+  if (c.maxb) g = std::min<uint64_t>(g, c.maxb);
+  return (unsigned)g;
+}
+
+int enqueue_persistent(mvbt_batch_plan* p, const launch_ctx& c, const batch_view& B, cudaStream_t s) {
+  const uint32_t mb = p->max_batches;
+  MVBT_TRY(cudaMemcpyAsync(p->d_batch_off, p->h_batch_off, (mb + 1) * sizeof(uint64_t),
+                           cudaMemcpyHostToDevice, s));
+  MVBT_TRY(cudaMemcpyAsync(p->d_params, p->h_params, 2 * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+  MVBT_TRY(cudaMemsetAsync(p->d_counts, 0, 4ull * mb * sizeof(uint32_t), s));
+  MVBT_TRY(cudaMemsetAsync(p->d_cursor, 0, sizeof(unsigned long long), s));
+  uint32_t* nw    = p->d_counts;
+  uint32_t* wdone = p->d_counts + mb;
+  uint32_t* wfill = p->d_counts + 2 * mb;
+  uint32_t* rfill = p->d_counts + 3 * mb;
+  k_count_writes<<<kPrepassBlocks, kPrepassThreads, 0, s>>>(B.type, p->d_batch_off, p->d_params, nw);
+  k_place<<<kPrepassBlocks, kPrepassThreads, 0, s>>>(B.type, p->d_batch_off, p->d_params, nw, wfill,
+                                                     rfill, p->d_perm);
+  k_batch_begin<<<1, 32, 0, s>>>(c.ctl, p->d_params);
+  batch_sched sc;
+  sc.batch_off   = p->d_batch_off;
+  sc.perm        = p->d_perm;
+  sc.n_writes    = nw;
+  sc.writes_done = wdone;
+  sc.cursor      = p->d_cursor;
+  sc.params      = p->d_params;
+  sc.chunk       = 16;
+  if (c.W == 8) {
+    k_batched<8><<<occupancy_grid(c, k_batched<8>), c.block, 0, s>>>(c.view, B, sc);
+  } else {
+    k_batched<16><<<occupancy_grid(c, k_batched<16>), c.block, 0, s>>>(c.view, B, sc);
+  }
+  k_batch_end<<<1, 32, 0, s>>>(c.ctl, p->d_params);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(MVBT_ERR_CUDA, std::string("batched launch: ") + cudaGetErrorString(e));
+  return MVBT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mvbt_batch_plan_create(mvbt_tree* tree, uint64_t max_ops, uint32_t max_batches,
+                           mvbt_batch_plan** out) {
+  if (!tree || !out || max_ops == 0 || max_batches == 0 || max_ops > 0xFFFFFFFFull)
+    return fail(MVBT_ERR_BAD_ARG, "bad batch plan arguments");
+  device_tree v;
+  int W, bs, sms;
+  uint32_t bps, maxb;
+  void* ctl;
+  int st = mvbt_internal_view(tree, &v, &W, &bs, &sms, &bps, &maxb, &ctl);
+  if (st) return st;
+  if (!v.versioned) return fail(MVBT_ERR_NOT_SUPPORTED, "mixed batches need a versioned tree");
+  auto* p        = new mvbt_batch_plan();
+  p->tree        = tree;
+  p->max_ops     = max_ops;
+  p->max_batches = max_batches;
+  bool ok = cudaMalloc(&p->d_batch_off, (max_batches + 1) * sizeof(uint64_t)) == cudaSuccess &&
+            cudaMalloc(&p->d_params, 64) == cudaSuccess &&
+            cudaMalloc(&p->d_perm, max_ops * sizeof(uint32_t)) == cudaSuccess &&
+            cudaMalloc(&p->d_counts, 4ull * max_batches * sizeof(uint32_t)) == cudaSuccess &&
+            cudaMalloc(&p->d_cursor, sizeof(unsigned long long)) == cudaSuccess &&
+            cudaMallocHost(&p->h_batch_off, (max_batches + 1) * sizeof(uint64_t)) == cudaSuccess &&
+            cudaMallocHost(&p->h_params, 64) == cudaSuccess;
+  if (!ok) {
+    cudaGetLastError();
+    mvbt_batch_plan_destroy(p);
+    return fail(MVBT_ERR_OUT_OF_MEMORY, "batch plan allocation failed");
+  }
+  *out = p;
+  return MVBT_OK;
+}
+
+int mvbt_batch_plan_destroy(mvbt_batch_plan* p) {
+  if (!p) return MVBT_OK;
+  cudaDeviceSynchronize();
+  if (p->have_graph) cudaGraphExecDestroy(p->graph);
+  cudaFree(p->d_batch_off);
+  cudaFree(p->d_params);
+  cudaFree(p->d_perm);
+  cudaFree(p->d_counts);
+  cudaFree(p->d_cursor);
+  cudaFreeHost(p->h_batch_off);
+  cudaFreeHost(p->h_params);
+  delete p;
+  return MVBT_OK;
+}
+
+int mvbt_batch_run(mvbt_batch_plan* p, uint32_t num_batches, const uint64_t* batch_off,
+                   const uint32_t* type, const uint32_t* key, const uint32_t* arg,
+                   const uint64_t* out_off, const uint32_t* range_cap, uint32_t* result,
+                   mvbt_pair* range_out, int mode, void* stream) {
+  if (!p || !batch_off || !type || !key || !arg || !result) return fail(MVBT_ERR_BAD_ARG, "null argument");
+  if (num_batches == 0) return MVBT_OK;
+  if (num_batches > p->max_batches) return fail(MVBT_ERR_BAD_ARG, "more batches than the plan holds");
+  const uint64_t total = batch_off[num_batches];
+  if (total > p->max_ops) return fail(MVBT_ERR_BAD_ARG, "more ops than the plan holds");
+  for (uint32_t b = 0; b < num_batches; ++b)
+    if (batch_off[b + 1] < batch_off[b]) return fail(MVBT_ERR_BAD_ARG, "batch offsets must not decrease");
+  if (batch_off[0] != 0) return fail(MVBT_ERR_BAD_ARG, "batch_off[0] must be 0");
+  launch_ctx c;
+  void* ctl;
+  int st = mvbt_internal_view(p->tree, &c.view, &c.W, &c.block, &c.sms, &c.bps, &c.maxb, &ctl);
+  if (st) return st;
+  c.ctl = static_cast<mvbt::control_block*>(ctl);
+  batch_view B;
+  B.type      = type;
+  B.key       = key;
+  B.arg       = arg;
+  B.out_off   = out_off;
+  B.cap       = range_cap;
+  B.result    = result;
+  B.range_out = reinterpret_cast<uint2*>(range_out);
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  if (total == 0) return MVBT_OK;
+
+  if (mode == MVBT_BATCH_PER_LAUNCH) {
+    // the plain method: per batch, one snapshot and one mixed launch
+    for (uint32_t b = 0; b < num_batches; ++b) {
+      const uint64_t lo = batch_off[b], hi = batch_off[b + 1];
+      k_snapshot_word<<<1, 32, 0, s>>>(c.ctl, p->d_params + 1);
+      if (hi == lo) continue;
+      uint64_t tiles = (hi - lo);
+      uint64_t need  = (tiles * c.W + c.block - 1) / c.block;
+      unsigned grid;
+      if (c.W == 8) grid = (unsigned)std::min<uint64_t>(need, occupancy_grid(c, k_mixed<8>));
+      else grid = (unsigned)std::min<uint64_t>(need, occupancy_grid(c, k_mixed<16>));
+      if (c.W == 8) k_mixed<8><<<grid, c.block, 0, s>>>(c.view, B, lo, hi, p->d_params + 1);
+      else k_mixed<16><<<grid, c.block, 0, s>>>(c.view, B, lo, hi, p->d_params + 1);
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(MVBT_ERR_CUDA, std::string("per-batch launch: ") + cudaGetErrorString(e));
+    return MVBT_OK;
+  }
+
+  // stage the batch list in pinned memory (the captured graph copies from here)
+  MVBT_TRY(cudaStreamSynchronize(s));  // the previous run may still read the staging area
+  std::memcpy(p->h_batch_off, batch_off, (num_batches + 1) * sizeof(uint64_t));
+  for (uint32_t b = num_batches + 1; b <= p->max_batches; ++b) p->h_batch_off[b] = total;
+  p->h_params[0] = num_batches;
+  p->h_params[1] = 0;
+
+  if (mode == MVBT_BATCH_PERSISTENT) return enqueue_persistent(p, c, B, s);
+  if (mode != MVBT_BATCH_GRAPH) return fail(MVBT_ERR_BAD_ARG, "unknown batch mode");
+
+  const void* key_now[8] = {type, key, arg, out_off, range_cap, result, range_out, stream};
+  if (!p->have_graph || std::memcmp(key_now, p->graph_key, sizeof(key_now)) != 0) {
+    if (p->have_graph) {
+      cudaGraphExecDestroy(p->graph);
+      p->have_graph = false;
+    }
+    cudaStream_t cap;
+    MVBT_TRY(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+    MVBT_TRY(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
+    int rs = enqueue_persistent(p, c, B, cap);
+    cudaGraph_t g;
+    cudaError_t e = cudaStreamEndCapture(cap, &g);
+    cudaStreamDestroy(cap);
+    if (rs) return rs;
+    if (e != cudaSuccess) return fail(MVBT_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&p->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return fail(MVBT_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+    p->have_graph = true;
+    std::memcpy(p->graph_key, key_now, sizeof(key_now));
+  }
+  MVBT_TRY(cudaGraphLaunch(p->graph, s));
+  return MVBT_OK;
+}
+
+}  // extern "C"

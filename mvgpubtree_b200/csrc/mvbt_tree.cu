@@ -33,6 +33,9 @@ struct mvbt_tree {
   int num_sms;
   uint32_t spin_limit;
   uint32_t chunk;
+  uint32_t blocks_per_sm;
+  uint32_t max_blocks;
+  uint32_t wait_ms;
   device_tree view() const {
     device_tree t;
     t.pool      = pool;
@@ -65,33 +68,8 @@ inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s
 // ----------------------------------------------------------------------------------------------
 __global__ void k_init(uint32_t* pool, control_block* c, uint32_t capacity, uint32_t chunk,
                        uint32_t spin_limit, uint32_t wait_ns) {
-  const int t = threadIdx.x;
-  if (t < 32) {
-    // root leaf: {0,0} tombstone, empty pairs, high = MAX, no sibling, ts 0, no older, level 0
-    uint32_t w;
-    if (t == 0 || t == 1) w = 0u;
-    else if (t < 28) w = mvbt::kEmptyKey;
-    else if (t == 28) w = mvbt::kEmptyKey;  // high key
-    else if (t == 29) w = mvbt::kNone;      // link
-    else if (t == 30) w = 0u;               // ts
-    else w = mvbt::kNone;                   // older | level 0
-    pool[t] = w;
-  }
-  if (t == 0) {
-    c->epoch         = 0;
-    c->error         = 0;
-    c->bump          = 1;
-    c->capacity      = capacity;
-    c->chunk         = chunk;
-    c->spin_limit    = spin_limit;
-    c->wait_ns       = wait_ns;
-    c->reserved      = 0;
-    c->stat_cow      = 0;
-    c->stat_split    = 0;
-    c->stat_restart  = 0;
-    c->stat_reserved = 0;
-  }
-  for (int i = t; i < mvbt::kMaxSmSlots; i += blockDim.x) c->sm_pool[i] = chunk;  // "used == chunk": refill first
+  if (threadIdx.x < 32) pool[threadIdx.x] = mvbt::initial_root_word(threadIdx.x);
+  if (threadIdx.x == 0) mvbt::init_control(*c, capacity, chunk, spin_limit, wait_ns);
 }
 
 __global__ void k_snapshot(control_block* c, uint32_t* out) {
@@ -220,10 +198,12 @@ unsigned grid_for(const mvbt_tree* t, K kernel, uint64_t ops) {
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, t->block_size, 0);
   if (per_sm < 1) per_sm = 1;
+  if (t->blocks_per_sm && (int)t->blocks_per_sm < per_sm) per_sm = (int)t->blocks_per_sm;
   uint64_t tiles_per_block = (uint64_t)t->block_size / t->tile_width;
   uint64_t need            = (ops + tiles_per_block - 1) / tiles_per_block;
   uint64_t cap             = (uint64_t)per_sm * t->num_sms;
   uint64_t g               = std::min<uint64_t>(std::max<uint64_t>(need, 1), cap);
+  if (t->max_blocks) g = std::min<uint64_t>(g, t->max_blocks);
   return (unsigned)g;
 }
 
@@ -239,21 +219,6 @@ int status_from_bits(uint32_t bits) {
   if (bits & (mvbt::kErrCorrupt | mvbt::kErrStepLimit)) return MVBT_ERR_CORRUPT;
   return MVBT_OK;
 }
-
-// ----------------------------------------------------------------------------------------------
-// Host structural walk over a pool image (the counterpart of validate_tree_structure)
-// ----------------------------------------------------------------------------------------------
-struct host_node {
-  const uint32_t* w;
-  uint32_t key(int p) const { return w[2 * p]; }
-  uint32_t val(int p) const { return w[2 * p + 1]; }
-  uint32_t high() const { return w[28]; }
-  uint32_t link() const { return w[29]; }
-  uint32_t ts() const { return w[30]; }
-  uint32_t level() const { return w[31] >> 28; }
-  uint32_t older() const { return w[31] & mvbt::kIndexMask; }
-  uint32_t sibling() const { return w[29] & mvbt::kIndexMask; }
-};
 
 }  // namespace
 
@@ -271,6 +236,7 @@ void mvbt_config_init(mvbt_config* cfg) {
   cfg->block_size  = 256;
   cfg->spin_limit  = 1u << 20;
   cfg->chunk_nodes = 64;
+  cfg->wait_ms     = 2000;
 }
 
 const char* mvbt_last_error(void) { return g_last_error.c_str(); }
@@ -320,8 +286,12 @@ int mvbt_create(int kind, const mvbt_config* cfg_in, mvbt_tree** out) {
   t->tile_width = cfg.tile_width;
   t->block_size = cfg.block_size;
   t->capacity   = capacity;
-  t->spin_limit = cfg.spin_limit;
-  t->chunk      = cfg.chunk_nodes;
+  t->spin_limit    = cfg.spin_limit;
+  t->chunk         = cfg.chunk_nodes;
+  t->blocks_per_sm = cfg.blocks_per_sm;
+  t->max_blocks    = cfg.max_blocks;
+  t->wait_ms       = cfg.wait_ms ? cfg.wait_ms : 2000u;
+  if (t->wait_ms > 4000u) t->wait_ms = 4000u;  // wait_ns is a 32-bit ns count
   cudaDeviceProp prop;
   cudaError_t e = cudaGetDeviceProperties(&prop, dev);
   if (e != cudaSuccess) {
@@ -341,7 +311,7 @@ int mvbt_create(int kind, const mvbt_config* cfg_in, mvbt_tree** out) {
     delete t;
     return fail(MVBT_ERR_OUT_OF_MEMORY, "cudaMalloc of the control block failed");
   }
-  k_init<<<1, 256>>>(t->pool, t->ctl, (uint32_t)capacity, t->chunk, t->spin_limit, 50u * 1000u * 1000u);
+  k_init<<<1, 256>>>(t->pool, t->ctl, (uint32_t)capacity, t->chunk, t->spin_limit, t->wait_ms * 1000000u);
   e = cudaDeviceSynchronize();
   if (e != cudaSuccess) {
     mvbt_destroy(t);
@@ -528,6 +498,36 @@ int mvbt_memory_usage(mvbt_tree* t, uint64_t* nodes, uint64_t* bytes, uint64_t* 
   return MVBT_OK;
 }
 
+int mvbt_copy_pool(mvbt_tree* t, void* dst, uint64_t max_nodes, uint64_t* nodes) {
+  if (!t || !dst) return fail(MVBT_ERR_BAD_ARG, "null argument");
+  MVBT_CUDA_TRY(cudaSetDevice(t->device));
+  MVBT_CUDA_TRY(cudaDeviceSynchronize());
+  uint32_t bump = 0;
+  MVBT_CUDA_TRY(cudaMemcpy(&bump, &t->ctl->bump, 4, cudaMemcpyDeviceToHost));
+  uint64_t nn = std::min<uint64_t>(std::min<uint64_t>(bump, t->capacity), max_nodes);
+  MVBT_CUDA_TRY(cudaMemcpy(dst, t->pool, nn * 128, cudaMemcpyDeviceToHost));
+  if (nodes) *nodes = nn;
+  return MVBT_OK;
+}
+
+// Internal accessors for the other translation units of the library.
+int mvbt_internal_view(mvbt_tree* t, device_tree* view, int* tile_width, int* block_size,
+                       int* num_sms, uint32_t* blocks_per_sm, uint32_t* max_blocks, void** control) {
+  if (!t) return fail(MVBT_ERR_BAD_ARG, "null tree");
+  cudaError_t e = cudaSetDevice(t->device);
+  if (e != cudaSuccess) return fail(MVBT_ERR_CUDA, cudaGetErrorString(e));
+  *view          = t->view();
+  *tile_width    = t->tile_width;
+  *block_size    = t->block_size;
+  *num_sms       = t->num_sms;
+  *blocks_per_sm = t->blocks_per_sm;
+  *max_blocks    = t->max_blocks;
+  *control       = t->ctl;
+  return MVBT_OK;
+}
+
+void mvbt_internal_set_error(const char* msg) { g_last_error = msg ? msg : ""; }
+
 int mvbt_get_device_view(mvbt_tree* t, mvbt_device_view* out) {
   if (!t || !out) return fail(MVBT_ERR_BAD_ARG, "null argument");
   out->pool      = t->pool;
@@ -547,93 +547,9 @@ int mvbt_validate(mvbt_tree* t, uint32_t ts, mvbt_report* rep) {
   uint64_t nn = std::min<uint64_t>(bump, t->capacity);
   std::vector<uint32_t> img(nn * 32);
   MVBT_CUDA_TRY(cudaMemcpy(img.data(), t->pool, nn * 128, cudaMemcpyDeviceToHost));
-  rep->nodes_allocated = nn;
-  const bool snap      = t->kind == MVBT_KIND_VERSIONED && ts != mvbt::kLatest;
-  auto node            = [&](uint32_t i) { return host_node{img.data() + (size_t)i * 32}; };
-  uint32_t violations  = 0;
-  auto resolve         = [&](uint32_t i) -> uint32_t {
-    uint32_t hops = 0;
-    while (snap && i < nn && node(i).ts() > ts) {
-      i = node(i).older();
-      if (++hops > 1000000) return mvbt::kNone;
-    }
-    return i < nn ? i : mvbt::kNone;
-  };
-  uint32_t root = resolve(mvbt::kRoot);
-  if (root == mvbt::kNone) {
-    rep->violations = 1;
-    return fail(MVBT_ERR_CORRUPT, "root version not found");
-  }
-  int top        = (int)node(root).level();
-  rep->height    = (uint32_t)top + 1;
-  uint32_t first = mvbt::kRoot;  // slot index of the leftmost node of the level
-  std::vector<uint32_t> child_slots;
-  for (int level = top; level >= 0; --level) {
-    std::vector<uint32_t> slots;
-    std::vector<uint32_t> next_children;
-    uint32_t slot = first, low = 0;
-    uint64_t guard = 0;
-    while (slot != mvbt::kNone) {
-      if (++guard > nn + 1) {
-        ++violations;
-        break;
-      }
-      uint32_t v = resolve(slot);
-      if (v == mvbt::kNone) {
-        ++violations;
-        break;
-      }
-      host_node x = node(v);
-      slots.push_back(slot);
-      if ((int)x.level() != level) ++violations;
-      if (x.link() & mvbt::kLockBit) ++rep->locked_nodes;
-      uint32_t prev = 0;
-      bool have     = false;
-      int cnt       = 0;
-      for (int p = 0; p < mvbt::kDataPairs; ++p) {
-        uint32_t k = x.key(p);
-        if (k == mvbt::kEmptyKey) {
-          for (int q = p; q < mvbt::kDataPairs; ++q)
-            if (x.key(q) != mvbt::kEmptyKey) ++violations;  // valid pairs form a prefix
-          break;
-        }
-        ++cnt;
-        if (have && k <= prev) ++violations;
-        if (k < low || k >= x.high()) ++violations;
-        prev = k;
-        have = true;
-        if (level == 0) {
-          ++rep->keys;
-          rep->key_checksum += (uint64_t)k * 0x9E3779B1ull + x.val(p);
-        } else {
-          next_children.push_back(x.val(p));
-        }
-      }
-      if (level > 0 && cnt == 0) ++violations;
-      if (level == 0) ++rep->leaves;
-      else ++rep->interior;
-      if (x.high() <= low && x.high() != mvbt::kEmptyKey) ++violations;
-      low  = x.high();
-      slot = x.sibling();
-      if (slot == mvbt::kNone && x.high() != mvbt::kEmptyKey) ++violations;
-    }
-    // every node of this level is referenced by exactly one parent entry
-    if (level < top) {
-      std::vector<uint32_t> a = slots, b = child_slots;
-      std::sort(a.begin(), a.end());
-      std::sort(b.begin(), b.end());
-      if (a != b) ++violations;
-    }
-    child_slots = next_children;
-    if (level > 0) {
-      uint32_t v = resolve(first);
-      if (v == mvbt::kNone) break;
-      first = node(v).val(0);
-    }
-  }
-  rep->violations = violations;
-  if (violations) return fail(MVBT_ERR_CORRUPT, "tree structure check failed: " + std::to_string(violations) + " violations");
-  return MVBT_OK;
+  int st = mvbt_validate_image(img.data(), nn, t->kind == MVBT_KIND_VERSIONED, ts, rep);
+  if (st) g_last_error = "tree structure check failed: " + std::to_string(rep->violations) + " violations";
+  return st;
 }
 
 }  // extern "C"

@@ -128,3 +128,44 @@ class GpuDriver:
         rep = self.tree.validate_tree_structure(ts)
         assert rep["keys"] == c, f"walk found {rep['keys']} keys, scan found {c}"
         return pairs[0, :c, 0].copy(), pairs[0, :c, 1].copy()
+
+
+class EmuDriver:
+    """The device tree code compiled for the host, W lanes per tile as threads (tests/emu)."""
+
+    def __init__(self, versioned: bool, tile_width: int = 8, tiles: int = 4, capacity: int = 1 << 15):
+        from emu import EmuTree
+        self.t = EmuTree(versioned, capacity=capacity, tiles=tiles, W=tile_width)
+
+    def _ok(self):
+        assert self.t.errors == 0, f"device error bits {self.t.errors}"
+
+    def insert(self, k, v, in_place=True):
+        self.t.insert(k, v)
+        self._ok()
+
+    def erase(self, k):
+        self.t.erase(k)
+        self._ok()
+
+    def snapshot(self):
+        return self.t.snapshot()
+
+    def find(self, k, ts):
+        r = self.t.find(k, ts)
+        self._ok()
+        return r
+
+    def range(self, lo, hi, avg_len, ts):
+        r = self.t.range(lo, hi, avg_len, ts)
+        self._ok()
+        return r
+
+    def contents(self, ts, expected=None):
+        cap = (expected or 0) + 64
+        pairs, counts = self.t.range([0], [SENTINEL], cap, ts)
+        c = int(counts[0])
+        rep = self.t.validate(ts)
+        assert rep["status"] == 0 and rep["violations"] == 0, rep
+        assert rep["keys"] == c and rep["locked_nodes"] == 0, rep
+        return pairs[0, :c, 0].copy(), pairs[0, :c, 1].copy()

@@ -1,0 +1,114 @@
+"""ctypes front-end of the CPU emulation harness (the device tree code compiled for the host)."""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from .build import LIB, build
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        _lib = ctypes.CDLL(str(LIB))
+        u32p = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
+        vp, u32, u64, i = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int
+        sig = {
+            "emu_create": (vp, [i, u32, u32, u32]),
+            "emu_destroy": (None, [vp]),
+            "emu_errors": (u32, [vp]),
+            "emu_bump": (u32, [vp]),
+            "emu_snapshot": (u32, [vp]),
+            "emu_insert": (None, [vp, u32p, u32p, u64, i, i]),
+            "emu_erase": (None, [vp, u32p, u64, i, i]),
+            "emu_find": (None, [vp, u32p, u32p, u64, u32, i, i]),
+            "emu_range": (None, [vp, u32p, u32p, vp, vp, u32, u64, u32, i, i]),
+            "emu_insert_range": (None, [vp, u32p, u32p, u64, u32p, u32p, u64, vp, vp, u32, i, i]),
+            "emu_validate": (i, [vp, u32, vp]),
+            "emu_batch_run": (None, [vp, u32, np.ctypeslib.ndpointer(dtype=np.uint64, flags="C_CONTIGUOUS"),
+                                     u32p, u32p, u32p,
+                                     np.ctypeslib.ndpointer(dtype=np.uint64, flags="C_CONTIGUOUS"),
+                                     u32p, u32p, vp, i, i, i]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(_lib, name)
+            f.restype = res
+            f.argtypes = args
+    return _lib
+
+
+def _u32(a):
+    return np.ascontiguousarray(a, dtype=np.uint32)
+
+
+class EmuTree:
+    """A tree held in host memory, operated on by the device code run as host threads."""
+
+    def __init__(self, versioned: bool, capacity: int = 1 << 16, tiles: int = 4, W: int = 8,
+                 spin_limit: int = 0, chunk: int = 8):
+        self.L = lib()
+        self.h = self.L.emu_create(int(versioned), capacity, spin_limit, chunk)
+        self.tiles, self.W = tiles, W
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.L.emu_destroy(self.h)
+            self.h = None
+
+    @property
+    def errors(self) -> int:
+        return int(self.L.emu_errors(self.h))
+
+    def snapshot(self) -> int:
+        return int(self.L.emu_snapshot(self.h))
+
+    def insert(self, k, v):
+        k, v = _u32(k), _u32(v)
+        self.L.emu_insert(self.h, k, v, k.size, self.tiles, self.W)
+
+    def erase(self, k):
+        k = _u32(k)
+        self.L.emu_erase(self.h, k, k.size, self.tiles, self.W)
+
+    def find(self, k, ts=0xFFFFFFFF):
+        k = _u32(k)
+        out = np.empty_like(k)
+        self.L.emu_find(self.h, k, out, k.size, ts, self.tiles, self.W)
+        return out
+
+    def range(self, lo, hi, avg_len, ts=0xFFFFFFFF):
+        lo, hi = _u32(lo), _u32(hi)
+        n = lo.size
+        pairs = np.full((n, avg_len, 2), 0xFFFFFFFF, np.uint32)
+        counts = np.zeros(n, np.uint32)
+        self.L.emu_range(self.h, lo, hi, pairs.ctypes.data, counts.ctypes.data, avg_len, n, ts,
+                         self.tiles, self.W)
+        return pairs, counts
+
+    def insert_range(self, k, v, lo, hi, avg_len):
+        k, v, lo, hi = _u32(k), _u32(v), _u32(lo), _u32(hi)
+        pairs = np.full((max(1, lo.size), avg_len, 2), 0xFFFFFFFF, np.uint32)
+        counts = np.zeros(max(1, lo.size), np.uint32)
+        self.L.emu_insert_range(self.h, k, v, k.size, lo, hi, lo.size, pairs.ctypes.data,
+                                counts.ctypes.data, avg_len, self.tiles, self.W)
+        return pairs[: lo.size], counts[: lo.size]
+
+    def run_batches(self, b, mode: int = 0):
+        """Runs mvgpubtree_b200.workload.Batches; returns (result, range_out words)."""
+        result = np.zeros(b.num_ops, np.uint32)
+        out = np.full(max(1, b.range_pairs) * 2, 0xFFFFFFFF, np.uint32)
+        self.L.emu_batch_run(self.h, b.num_batches, b.batch_off, b.type, b.key, b.arg, b.out_off,
+                             b.range_cap, result, out.ctypes.data, mode, self.tiles, self.W)
+        return result, out
+
+    def validate(self, ts=0xFFFFFFFF) -> dict:
+        import mvgpubtree_b200 as mv
+        rep = mv.mvbt_report()
+        st = self.L.emu_validate(self.h, ts, ctypes.byref(rep))
+        out = {f: getattr(rep, f) for f, _ in mv.mvbt_report._fields_ if not f.startswith("reserved")}
+        out["status"] = st
+        return out

@@ -1,0 +1,224 @@
+// CPU emulation harness for the device tree (test infrastructure).
+//
+// Compiles include/mvbt_device.cuh for the host (MVBT_HOST_EMULATION) and runs every W-lane tile
+// as W host threads: shfl / ballot / sync go through a per-tile exchange buffer and a barrier,
+// atomics are GCC atomics on the shared pool. Several tiles run at once, so the lock, split and
+// versioning protocols are exercised concurrently on the CPU before any GPU run.
+#define MVBT_HOST_EMULATION 1
+#include <barrier>
+#include <cstdint>
+#include <cstring>
+#include <functional>
+#include <memory>
+#include <thread>
+#include <vector>
+
+#include "mvbt.h"
+#include "mvbt_device.cuh"
+
+namespace {
+
+struct tile_shared {
+  std::barrier<> bar;
+  uint64_t slot[32];
+  explicit tile_shared(int w) : bar(w) {}
+};
+
+// Emulated cooperative-groups tile of W lanes.
+struct emu_tile {
+  int rank;
+  int W;
+  tile_shared* sh;
+  int thread_rank() const { return rank; }
+  void sync() const { sh->bar.arrive_and_wait(); }
+  template <class T>
+  T shfl(T v, int src) const {
+    sh->slot[rank] = (uint64_t)v;
+    sync();
+    T r = (T)sh->slot[((src % W) + W) % W];
+    sync();
+    return r;
+  }
+  unsigned ballot(int p) const {
+    sh->slot[rank] = p ? 1u : 0u;
+    sync();
+    unsigned m = 0;
+    for (int i = 0; i < W; ++i)
+      if (sh->slot[i]) m |= 1u << i;
+    sync();
+    return m;
+  }
+};
+
+struct emu_tree {
+  std::vector<uint32_t> pool;
+  mvbt::control_block ctl;
+  uint32_t capacity;
+  int versioned;
+  mvbt::device_tree view() {
+    mvbt::device_tree t;
+    t.pool      = pool.data();
+    t.ctl       = &ctl;
+    t.versioned = (uint32_t)versioned;
+    t.capacity  = capacity;
+    return t;
+  }
+};
+
+// Runs op(i, tile) for i in [0, n) over `tiles` concurrent tiles of W threads (grid-stride).
+void run(uint64_t n, int tiles, int W, const std::function<void(uint64_t, const emu_tile&)>& op) {
+  if (n == 0) return;
+  if (tiles < 1) tiles = 1;
+  std::vector<std::unique_ptr<tile_shared>> sh;
+  for (int t = 0; t < tiles; ++t) sh.emplace_back(new tile_shared(W));
+  std::vector<std::thread> th;
+  for (int t = 0; t < tiles; ++t) {
+    for (int l = 0; l < W; ++l) {
+      th.emplace_back([&, t, l] {
+        mvbt::emu::sm = (uint32_t)t;
+        emu_tile tile{l, W, sh[t].get()};
+        for (uint64_t i = (uint64_t)t; i < n; i += (uint64_t)tiles) op(i, tile);
+      });
+    }
+  }
+  for (auto& x : th) x.join();
+}
+
+}  // namespace
+
+extern "C" {
+
+void* emu_create(int versioned, uint32_t capacity, uint32_t spin_limit, uint32_t chunk) {
+  auto* t      = new emu_tree();
+  t->capacity  = capacity;
+  t->versioned = versioned;
+  t->pool.assign((size_t)capacity * 32, 0xA5A5A5A5u);  // garbage, as fresh cudaMalloc memory
+  for (int i = 0; i < 32; ++i) t->pool[i] = mvbt::initial_root_word(i);
+  mvbt::init_control(t->ctl, capacity, chunk ? chunk : 8, spin_limit ? spin_limit : (1u << 20),
+                     200u * 1000u * 1000u);
+  return t;
+}
+
+void emu_destroy(void* h) { delete static_cast<emu_tree*>(h); }
+
+uint32_t emu_errors(void* h) { return static_cast<emu_tree*>(h)->ctl.error; }
+uint32_t emu_bump(void* h) { return static_cast<emu_tree*>(h)->ctl.bump; }
+
+uint32_t emu_snapshot(void* h) {
+  auto* t = static_cast<emu_tree*>(h);
+  return __atomic_fetch_add(&t->ctl.epoch, 1u, __ATOMIC_SEQ_CST);
+}
+
+#define EMU_DISPATCH(W, BODY)                    \
+  if (W == 8) {                                  \
+    constexpr int kW = 8;                        \
+    BODY;                                        \
+  } else {                                       \
+    constexpr int kW = 16;                       \
+    BODY;                                        \
+  }
+
+void emu_insert(void* h, const uint32_t* keys, const uint32_t* vals, uint64_t n, int tiles, int W) {
+  auto* t = static_cast<emu_tree*>(h);
+  auto v  = t->view();
+  EMU_DISPATCH(W, run(n, tiles, kW, [&](uint64_t i, const emu_tile& tile) {
+    uint32_t E = v.versioned ? v.current_epoch() : 0u;
+    v.cooperative_insert<kW>(keys[i], vals[i], tile, E);
+  }));
+}
+
+void emu_erase(void* h, const uint32_t* keys, uint64_t n, int tiles, int W) {
+  auto* t = static_cast<emu_tree*>(h);
+  auto v  = t->view();
+  EMU_DISPATCH(W, run(n, tiles, kW, [&](uint64_t i, const emu_tile& tile) {
+    uint32_t E = v.versioned ? v.current_epoch() : 0u;
+    v.cooperative_erase<kW>(keys[i], tile, E);
+  }));
+}
+
+void emu_find(void* h, const uint32_t* keys, uint32_t* out, uint64_t n, uint32_t ts, int tiles, int W) {
+  auto* t = static_cast<emu_tree*>(h);
+  auto v  = t->view();
+  if (!v.versioned) ts = mvbt::kLatest;
+  EMU_DISPATCH(W, run(n, tiles, kW, [&](uint64_t i, const emu_tile& tile) {
+    uint32_t r = v.cooperative_find<kW>(keys[i], tile, ts, true);
+    if (tile.thread_rank() == 0) out[i] = r;
+  }));
+}
+
+void emu_range(void* h, const uint32_t* lo, const uint32_t* hi, uint32_t* pairs, uint32_t* counts,
+               uint32_t avg_len, uint64_t n, uint32_t ts, int tiles, int W) {
+  auto* t = static_cast<emu_tree*>(h);
+  auto v  = t->view();
+  if (!v.versioned) ts = mvbt::kLatest;
+  EMU_DISPATCH(W, run(n, tiles, kW, [&](uint64_t i, const emu_tile& tile) {
+    uint2* o   = pairs ? reinterpret_cast<uint2*>(pairs) + i * (uint64_t)avg_len : nullptr;
+    uint32_t c = v.cooperative_range_query<kW>(lo[i], hi[i], tile, ts, o, avg_len, true);
+    if (counts && tile.thread_rank() == 0) counts[i] = c;
+  }));
+}
+
+// One run mixing inserts and range queries; queries read snapshot S, inserts land in S + 1.
+void emu_insert_range(void* h, const uint32_t* keys, const uint32_t* vals, uint64_t n_ins,
+                      const uint32_t* lo, const uint32_t* hi, uint64_t n_rq, uint32_t* pairs,
+                      uint32_t* counts, uint32_t avg_len, int tiles, int W) {
+  auto* t          = static_cast<emu_tree*>(h);
+  auto v           = t->view();
+  const uint32_t S = v.versioned ? emu_snapshot(h) : mvbt::kLatest;
+  const uint32_t E = v.versioned ? S + 1 : 0u;
+  const uint64_t total = n_ins + n_rq;
+  EMU_DISPATCH(W, run(total, tiles, kW, [&](uint64_t i, const emu_tile& tile) {
+    uint64_t a = (i * n_ins) / total, b = ((i + 1) * n_ins) / total;
+    if (b > a) {
+      v.cooperative_insert<kW>(keys[a], vals[a], tile, E);
+    } else {
+      uint64_t r = i - a;
+      uint2* o   = pairs ? reinterpret_cast<uint2*>(pairs) + r * (uint64_t)avg_len : nullptr;
+      uint32_t c = v.cooperative_range_query<kW>(lo[r], hi[r], tile, S, o, avg_len, true);
+      if (counts && tile.thread_rank() == 0) counts[r] = c;
+    }
+  }));
+}
+
+// Mixed batches. mode 0: the persistent worker loop (claim order writes-first per batch, batch b
+// waits for the writes of batch b - 1); mode 1: one snapshot + one run per batch.
+void emu_batch_run(void* h, uint32_t nb, const uint64_t* off, const uint32_t* type, const uint32_t* key,
+                   const uint32_t* arg, const uint64_t* out_off, const uint32_t* cap, uint32_t* result,
+                   uint32_t* range_out, int mode, int tiles, int W) {
+  auto* t = static_cast<emu_tree*>(h);
+  auto v  = t->view();
+  mvbt::batch_view B{type, key, arg, out_off, cap, result, reinterpret_cast<uint2*>(range_out)};
+  if (mode == 1) {
+    for (uint32_t b = 0; b < nb; ++b) {
+      uint32_t S = emu_snapshot(h);
+      uint64_t lo = off[b], n = off[b + 1] - off[b];
+      EMU_DISPATCH(W, run(n, tiles, kW, [&](uint64_t i, const emu_tile& tile) {
+        mvbt::run_batch_op<kW>(v, B, lo + i, S, S + 1, tile);
+      }));
+    }
+    return;
+  }
+  std::vector<uint32_t> perm(off[nb]), n_writes(nb, 0), writes_done(nb, 0);
+  for (uint32_t b = 0; b < nb; ++b) {
+    uint64_t pos = off[b];
+    for (uint64_t i = off[b]; i < off[b + 1]; ++i)
+      if (mvbt::is_write_op(type[i])) perm[pos++] = (uint32_t)i, ++n_writes[b];
+    for (uint64_t i = off[b]; i < off[b + 1]; ++i)
+      if (!mvbt::is_write_op(type[i])) perm[pos++] = (uint32_t)i;
+  }
+  unsigned long long cursor = 0;
+  uint32_t params[2]        = {nb, t->ctl.epoch};
+  mvbt::batch_sched sc{off, perm.data(), n_writes.data(), writes_done.data(), &cursor, params, 4};
+  EMU_DISPATCH(W, run((uint64_t)tiles, tiles, kW, [&](uint64_t, const emu_tile& tile) {
+    mvbt::batched_worker<kW>(v, B, sc, tile);
+  }));
+  t->ctl.epoch = params[1] + nb;
+}
+
+int emu_validate(void* h, uint32_t ts, mvbt_report* rep) {
+  auto* t     = static_cast<emu_tree*>(h);
+  uint64_t nn = std::min<uint64_t>(t->ctl.bump, t->capacity);
+  return mvbt_validate_image(t->pool.data(), nn, t->versioned, ts, rep);
+}
+
+}  // extern "C"

@@ -1,0 +1,110 @@
+"""CPU tier: the device tree code (include/mvbt_device.cuh) compiled for the host and run with
+W host threads per tile and several concurrent tiles (tests/emu), checked against the oracle.
+
+This exercises the lock, split, copy-on-write and snapshot-read protocols on the CPU; the GPU
+tier repeats the same checks on the B200.
+"""
+import numpy as np
+import pytest
+
+from cases import EmuDriver, load_cases, replay
+
+
+def _case_params():
+    _, index = load_cases()
+    out = []
+    for c in index:
+        for kind in c["kinds"]:
+            out.append(pytest.param(c["name"], kind, 8, id=f"{c['name']}-{kind}-w8"))
+    # W=16 on a representative subset to keep the CPU tier short
+    for name, kind in (("btree_EraseAllInsertAllTest", "versioned"), ("versioning_RangeQueryTest", "versioned"),
+                       ("find_blink_test", "blink")):
+        out.append(pytest.param(name, kind, 16, id=f"{name}-{kind}-w16"))
+    return out
+
+
+@pytest.mark.parametrize("name,kind,w", _case_params())
+def test_emulated_tree_matches_reference_known_answers(name, kind, w):
+    z, index = load_cases()
+    case = next(c for c in index if c["name"] == name)
+    replay(EmuDriver(kind == "versioned", tile_width=w, tiles=8), z, case)
+
+
+@pytest.mark.parametrize("w", [8, 16])
+def test_emulated_concurrent_insert_range_at_launch_snapshot(w):
+    from emu import EmuTree
+    from mvgpubtree_b200 import workload as wl
+    import oracle
+    seed, n0, L = 3, 3000, 8
+    keys = wl.distinct_keys(seed, 0, n0)
+    vals = wl.values_for(keys, seed)
+    t = EmuTree(True, capacity=1 << 15, tiles=8, W=w)
+    m = oracle.MVMap(True)
+    t.insert(keys, vals)
+    m.insert(keys, vals)
+    ins = wl.distinct_keys(seed, n0, 1500)
+    lo = wl.uniform_keys(seed, 600)
+    hi = wl.upper_bounds(lo, L, wl.stride_for(n0))
+    pairs, counts = t.insert_range(ins, wl.values_for(ins, seed), lo, hi, 32)
+    assert t.errors == 0
+    s = m.take_snapshot()
+    ep, ec = m.range_query(lo, hi, 32, s)
+    assert np.array_equal(counts, ec)
+    mask = np.arange(32)[None, :] < np.minimum(ec, 32)[:, None]
+    assert np.array_equal(pairs[mask], ep[mask])
+    m.insert(ins, wl.values_for(ins, seed))
+    q = np.concatenate([keys, ins])
+    assert np.array_equal(t.find(q), m.find(q))
+    rep = t.validate()
+    assert rep["violations"] == 0 and rep["locked_nodes"] == 0 and rep["keys"] == n0 + 1500 + 1
+    rep0 = t.validate(s)
+    assert rep0["violations"] == 0 and rep0["keys"] == n0 + 1
+
+
+def test_emulated_updates_erases_keep_old_snapshots():
+    from emu import EmuTree
+    from mvgpubtree_b200 import workload as wl
+    import oracle
+    seed, n0 = 9, 4000
+    keys = wl.distinct_keys(seed, 0, n0)
+    t = EmuTree(True, capacity=1 << 15, tiles=8, W=8)
+    m = oracle.MVMap(True)
+    t.insert(keys, wl.values_for(keys, seed)); m.insert(keys, wl.values_for(keys, seed))
+    snaps = []
+    for r in range(3):
+        snaps.append(t.snapshot()); m.take_snapshot()
+        upd = wl.shuffle(seed + r, keys)[:800]
+        t.insert(upd, wl.values_for(upd, seed + 100 + r)); m.insert(upd, wl.values_for(upd, seed + 100 + r))
+        er = wl.shuffle(seed + 50 + r, keys)[:300]
+        t.erase(er); m.erase(er)
+        more = wl.distinct_keys(seed, n0 + 1000 * r, 500)
+        t.insert(more, wl.values_for(more, seed)); m.insert(more, wl.values_for(more, seed))
+    assert t.errors == 0
+    q = np.concatenate([keys, wl.distinct_keys(seed, n0, 3000)])
+    for s in snaps + [0xFFFFFFFF]:
+        assert np.array_equal(t.find(q, s), m.find(q, s)), f"snapshot {s}"
+        assert t.validate(s)["violations"] == 0
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+@pytest.mark.parametrize("w", [8, 16])
+def test_emulated_mixed_batches_match_oracle(mode, w):
+    """Mixed erase/insert/find/range batches, one snapshot per batch (persistent worker loop
+    with the writes-of-previous-batch dependency, and the per-batch mode)."""
+    from emu import EmuTree
+    from mvgpubtree_b200 import workload as wl
+    import oracle
+    seed, n0 = 12, 4000
+    gen = wl.MixGenerator(seed, n0, stride=wl.stride_for(n0), batch_median=250, batch_min=1,
+                          batch_max=2500, batch_sigma=1.2)
+    b = gen.generate(12)
+    init = wl.distinct_keys(seed, 0, n0)
+    t = EmuTree(True, capacity=1 << 15, tiles=8, W=w)
+    m = oracle.MVMap(True)
+    t.insert(init, wl.values_for(init, 0))
+    m.insert(init, wl.values_for(init, 0))
+    r, o = t.run_batches(b, mode)
+    er, eo = m.run_batches(b)
+    assert t.errors == 0
+    assert np.array_equal(r, er) and np.array_equal(o, eo)
+    assert t.validate()["violations"] == 0
