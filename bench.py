@@ -1,0 +1,449 @@
+#!/usr/bin/env python
+"""Benchmark: mixed-op batches on a 40M-key multiversion B-link tree (one B200 per rank).
+
+Workload (one step): 256 independent batches of mixed ops -- erase 10 % (present keys),
+insert 20 % (new keys), find 50 % (half hits), range query 20 % (length L geometric with mean 32,
+clipped to [1, 1024], upper bound = lower + L * 107) -- with lognormal batch sizes (median 16K ops,
+sigma 1.5, clipped to [1K, 4M]), on a versioned tree that starts with 40M distinct uniform keys
+from [1, 2^32 - 3], one snapshot per batch. Inputs are synthetic and seeded (no dataset exists
+for this workload); each step gets fresh batches, generated against the evolving key set.
+
+value    : Mops/s of the batched path (one persistent launch per step, ops resident in HBM).
+e2e      : Mops/s through the public batch API with host buffers: per step the op arrays are
+           copied from pinned host memory, the captured CUDA graph is replayed and the results
+           (values, counts and range-output slots) are copied back.
+plain    : the same batches as one snapshot + one launch per batch (the drop-in method).
+roofline : algorithmic bytes of the persistent kernel per launch / its CUDA-event time.
+
+With --impl reference the script times the reference-side CPU implementation of the path (the
+oracle's multiversion ordered map, key-range partitioned over all host cores) on a bounded
+sample of every step of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Mops/s mixed ops @40M keys, batched vs plain launch, bit-exact; serving p99 µs"
+UNIT = "Mops/s"
+KEYS_40M = 40_000_000
+HBM_FALLBACK_GBS = 6650.0
+
+
+def parse_args():
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--initial-keys", type=int, default=KEYS_40M)
+    ap.add_argument("--batches", type=int, default=256)
+    ap.add_argument("--seed", type=int, default=20240611)
+    ap.add_argument("--tile-width", type=int, default=8)
+    ap.add_argument("--plain-steps", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--pool-gb", type=float, default=24.0)
+    ap.add_argument("--cpu-sample-ops", type=int, default=4_000_000,
+                    help="ops of the bounded CPU-baseline sample per step")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------------------------------------
+# process group (one process per GPU; replicas: no data-path collective)
+# ------------------------------------------------------------------------------------------------
+class Dist:
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+
+    def init(self, backend):
+        if self.world > 1:
+            import datetime
+            import torch.distributed as td
+            os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+            td.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+            self.pg = td
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, x: float) -> float:
+        if not self.pg:
+            return x
+        import torch
+        dev = "cuda" if self.pg.get_backend() == "nccl" else "cpu"
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+# ------------------------------------------------------------------------------------------------
+# clocks during the timed region
+# ------------------------------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+        self.reader = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.reader = threading.Thread(target=self._read, daemon=True)
+            self.reader.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.reader.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_hbm_gbs():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return HBM_FALLBACK_GBS, "fallback"
+
+
+# ------------------------------------------------------------------------------------------------
+# workload
+# ------------------------------------------------------------------------------------------------
+def make_workload(seed: int, initial: int, steps: int, batches: int):
+    from mvgpubtree_b200 import workload as wl
+    t0 = time.time()
+    init = wl.distinct_keys(seed, 0, initial)
+    vals = wl.values_for(init, 0)
+    gen = wl.MixGenerator(seed, initial, stride=wl.stride_for(KEYS_40M))
+    out = [gen.generate(batches) for _ in range(steps)]
+    return init, vals, out, time.time() - t0
+
+
+def op_bytes(b, result: np.ndarray, height: int, leaf_fill: float) -> float:
+    """Algorithmic bytes touched by one step's ops (node = 128 B, H = tree height):
+    find 128 H + 8; insert 128 (H + 1) + 256 + 8 (descent, locked reload, version copy, leaf
+    write, key + value); erase 128 (H + 1) + 256 + 4; range 128 H + 128 (leaves - 1) + 8 count + 8
+    with leaves = 1 + count / (keys per leaf)."""
+    t = b.type
+    n_find = int(np.count_nonzero(t == 0))
+    n_ins = int(np.count_nonzero(t == 1))
+    n_er = int(np.count_nonzero(t == 2))
+    cnt = result[t == 3].astype(np.float64)
+    H = float(height)
+    total = n_find * (128 * H + 8) + n_ins * (128 * (H + 1) + 256 + 8) + n_er * (128 * (H + 1) + 256 + 4)
+    total += float(np.sum(128 * H + 128 * (cnt / leaf_fill) + 8 * cnt + 8))
+    return total
+
+
+def run_ours(args, dist: Dist):
+    import torch
+    import mvgpubtree_b200 as mv
+
+    torch.cuda.set_device(dist.local)
+    dist.init("nccl")
+    seed = args.seed + 7919 * dist.rank
+    W, K = max(3, args.warmup), args.steps
+    Wp, Kp = 1, max(1, args.plain_steps)
+    We, Ke = 1, max(1, args.e2e_steps)
+    n_steps = max(W + K, Wp + Kp) + We + Ke
+    init, vals, steps, gen_s = make_workload(seed, args.initial_keys, n_steps, args.batches)
+
+    def dev(a):
+        a = np.ascontiguousarray(a)
+        if a.dtype == np.uint64:
+            return torch.from_numpy(a.view(np.int64)).cuda()
+        return torch.from_numpy(a.view(np.int32)).cuda()
+
+    pool = int(args.pool_gb * (1 << 30))
+    max_ops = max(b.num_ops for b in steps)
+    max_pairs = max(b.range_pairs for b in steps)
+    trees = {}
+    for name in ("batched", "plain"):
+        t = mv.gpu_versioned_btree(pool_bytes=pool, tile_width=args.tile_width)
+        t.insert(dev(init), dev(vals))
+        t.check_errors()
+        trees[name] = t
+    torch.cuda.synchronize()
+    plans = {k: t.batch_plan(max_ops, args.batches) for k, t in trees.items()}
+    range_out = torch.empty(max(1, max_pairs) * 2, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    # ---- batched, device-resident: W warm-up + K timed steps, one persistent launch each ----
+    dsteps = [[dev(b.type), dev(b.key), dev(b.arg), dev(b.out_off), dev(b.range_cap)] for b in steps[: W + K]]
+    results = [torch.empty(b.num_ops, dtype=torch.int32, device="cuda") for b in steps[: W + K]]
+    plan = plans["batched"]
+    for s in range(W):
+        plan.run(steps[s].batch_off, *dsteps[s], results[s], range_out, mode=mv.BATCH_PERSISTENT)
+    trees["batched"].check_errors()
+    plan.enable_timing(True)
+    clocks = ClockSampler(dist.local)
+    clocks.start()
+    dist.barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for s in range(W, W + K):
+        plan.run(steps[s].batch_off, *dsteps[s], results[s], range_out, mode=mv.BATCH_PERSISTENT)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    dist.barrier()
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    kernel_ms = plan.kernel_times()
+    plan.enable_timing(False)
+    trees["batched"].check_errors()
+    ops_timed = sum(steps[s].num_ops for s in range(W, W + K))
+    ms_max = dist.max(ms)
+    ops_all = ops_timed * dist.world
+    value = ops_all / (ms_max * 1e-3) / 1e6
+
+    # ---- plain: one snapshot + one launch per batch, same batches on an identical tree ----
+    pplan = plans["plain"]
+    for s in range(Wp):
+        pplan.run(steps[s].batch_off, *dsteps[s], results[s], range_out, mode=mv.BATCH_PER_LAUNCH)
+    dist.barrier()
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for s in range(Wp, Wp + Kp):
+        pplan.run(steps[s].batch_off, *dsteps[s], results[s], range_out, mode=mv.BATCH_PER_LAUNCH)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    trees["plain"].check_errors()
+    plain_ms = dist.max(ev0.elapsed_time(ev1))
+    plain_ops = sum(steps[s].num_ops for s in range(Wp, Wp + Kp)) * dist.world
+    plain_value = plain_ops / (plain_ms * 1e-3) / 1e6
+
+    # range counts of the timed steps (for the roofline bytes), read after the timed region
+    host_res = [results[s].cpu().numpy().view(np.uint32) for s in range(W, W + K)]
+    del dsteps, results
+    torch.cuda.empty_cache()
+
+    # ---- e2e: public API with pinned host buffers, CUDA graph replay ----
+    e2e_steps = steps[max(W + K, Wp + Kp):]
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.int64 if a.dtype == np.uint64 else np.int32)).pin_memory()
+    d_ops = [torch.empty(max_ops, dtype=torch.int32, device="cuda") for _ in range(3)]
+    d_off = torch.empty(max_ops, dtype=torch.int64, device="cuda")
+    d_cap = torch.empty(max_ops, dtype=torch.int32, device="cuda")
+    d_res = torch.empty(max_ops, dtype=torch.int32, device="cuda")
+    h_res = torch.empty(max_ops, dtype=torch.int32).pin_memory()
+    h_rout = torch.empty(max(1, max_pairs) * 2, dtype=torch.int32).pin_memory()
+    h_in = [[pin(b.type), pin(b.key), pin(b.arg), pin(b.out_off), pin(b.range_cap)] for b in e2e_steps]
+    h2d = d2h = 0
+    e2e_ms = 0.0
+    for s, b in enumerate(e2e_steps):
+        n = b.num_ops
+        if s == We:
+            dist.barrier()
+            torch.cuda.synchronize()
+            ev0.record(stream)
+        dst = [d_ops[0][:n], d_ops[1][:n], d_ops[2][:n], d_off[:n], d_cap[:n]]
+        for d, h in zip(dst, h_in[s]):
+            d.copy_(h, non_blocking=True)
+        plan.run(b.batch_off, d_ops[0], d_ops[1], d_ops[2], d_off, d_cap, d_res, range_out,
+                 mode=mv.BATCH_GRAPH, stream=stream)
+        h_res[:n].copy_(d_res[:n], non_blocking=True)
+        h_rout[: 2 * b.range_pairs].copy_(range_out[: 2 * b.range_pairs], non_blocking=True)
+        if s >= We:
+            h2d += sum(int(h.numel() * h.element_size()) for h in h_in[s])
+            d2h += n * 4 + b.range_pairs * 8
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    trees["batched"].check_errors()
+    e2e_ms = dist.max(ev0.elapsed_time(ev1))
+    e2e_ops = sum(b.num_ops for b in e2e_steps[We:]) * dist.world
+    e2e_value = e2e_ops / (e2e_ms * 1e-3) / 1e6
+
+    # ---- roofline of the persistent kernel ----
+    rep = trees["batched"].validate_tree_structure()
+    fill = rep["keys"] / max(1, rep["leaves"])
+    bytes_per = [op_bytes(steps[W + i], host_res[i], rep["height"], fill) for i in range(K)]
+    kms = kernel_ms[-K:] if len(kernel_ms) >= K else kernel_ms
+    avg_bytes = sum(bytes_per) / len(bytes_per)
+    avg_kms = sum(kms) / len(kms)
+    peak, peak_kind = measured_hbm_gbs()
+    achieved = avg_bytes / (avg_kms * 1e-3) / 1e9
+    traffic = None
+    tf = ROOT / "profiles" / "k_batched_traffic.json"
+    if tf.exists():
+        try:
+            traffic = json.loads(tf.read_text()).get("dram_bytes_per_launch")
+        except Exception:
+            traffic = None
+    mean_ops = sum(steps[s].num_ops for s in range(W, W + K)) / K
+    out = {
+        "metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": dist.world,
+        "steps": K, "warmup": W, "ms_per_step": round(ms_max / K, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded)",
+        "config": {
+            "workload": "mixed batches (erase 10 %, insert 20 %, find 50 % with 50 % hits, range "
+                        "20 % with L~geometric(32) clipped [1,1024], stride 107) on a 40M-key "
+                        "versioned B-link tree, one snapshot per batch",
+            "initial_keys": args.initial_keys, "batches_per_step": args.batches,
+            "batch_size": "lognormal median 16384, sigma 1.5, clipped [1024, 4194304]",
+            "mean_ops_per_step": int(mean_ops), "mode": "persistent launch, device work queue",
+            "tile_width": args.tile_width, "parallelism": f"replicas x{dist.world}",
+            "l2": "inputs larger than L2 (tree of %d nodes = %.1f GB; ops %.0f MB per step)" % (
+                rep["nodes_allocated"], rep["nodes_allocated"] * 128 / 1e9, mean_ops * 24 / 1e6),
+            "tree_height": rep["height"], "workload_gen_s": round(gen_s, 1),
+        },
+        "plain_per_batch": {"value": round(plain_value, 2), "unit": UNIT, "steps": Kp,
+                            "ms_per_step": round(plain_ms / Kp, 3),
+                            "batched_over_plain": round(value / plain_value, 3)},
+        "e2e": {"value": round(e2e_value, 2), "unit": UNIT,
+                "h2d_bytes_per_step": int(h2d / max(1, Ke)), "d2h_bytes_per_step": int(d2h / max(1, Ke)),
+                "mode": "CUDA graph replay via the public batch API, pinned host buffers"},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": traffic,
+                     "kernel": "k_batched", "kernel_ms": round(avg_kms, 3),
+                     "algorithmic_bytes_per_launch": int(avg_bytes), "peak_source": peak_kind},
+        "clocks": clk,
+        "gpu_launches": 5 * K,
+    }
+    return out, (init, vals, steps[W])
+
+
+# ------------------------------------------------------------------------------------------------
+# CPU side: the oracle (the reference-side CPU implementation of the path), timed on host cores
+# ------------------------------------------------------------------------------------------------
+def _sample(b, max_ops: int):
+    """The first batches of step b holding at most max_ops ops (at least one batch)."""
+    from mvgpubtree_b200.workload import Batches
+    nb = 1
+    while nb < b.num_batches and int(b.batch_off[nb + 1]) <= max_ops:
+        nb += 1
+    end = int(b.batch_off[nb])
+    r = b.type[:end] == 3
+    return Batches(b.batch_off[: nb + 1].copy(), b.type[:end], b.key[:end], b.arg[:end],
+                   b.out_off[:end], b.range_cap[:end],
+                   int((b.out_off[:end][r] + b.range_cap[:end][r]).max()) if r.any() else 0)
+
+
+def cpu_oracle_time(init, vals, batches, max_ops: int):
+    """Builds the partitioned oracle (untimed) and times its run of each sampled batch list."""
+    import oracle
+    cores = os.cpu_count() or 1
+    m = oracle.PartitionedMVMap(cores, versioned=True)
+    t0 = time.time()
+    m.insert(init, vals)
+    build_s = time.time() - t0
+    times, ops = [], []
+    for b in batches:
+        s = _sample(b, max_ops)
+        t0 = time.perf_counter()
+        m.run_batches(s, with_pairs=True)
+        times.append(time.perf_counter() - t0)
+        ops.append(s.num_ops)
+    m.close()
+    return cores, build_s, times, ops
+
+
+def run_reference(args, dist: Dist):
+    """Reference arm: the CPU implementation on the box's host cores (rank 0 only)."""
+    if dist.rank != 0:
+        return None
+    W, K = max(3, args.warmup), args.steps
+    init, vals, steps, _ = make_workload(args.seed, args.initial_keys, W + K, args.batches)
+    cores, build_s, times, ops = cpu_oracle_time(init, vals, steps, args.cpu_sample_ops)
+    t = sum(times[W:])
+    n = sum(ops[W:])
+    value = n / t / 1e6
+    sample = (f"first batches of each step up to {args.cpu_sample_ops} ops (mean "
+              f"{int(n / K)} ops/step) on the 40M-key map; build {build_s:.1f} s untimed")
+    return {
+        "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": UNIT,
+        "n_gpus": dist.world, "steps": K, "warmup": W, "ms_per_step": round(1e3 * t / K, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+        "data": "synthetic (seeded)",
+        "config": {"workload": "mixed batches on a 40M-key versioned tree, one snapshot per batch "
+                               "(same generator and seed as the GPU arm)",
+                   "initial_keys": args.initial_keys, "batches_per_step": args.batches,
+                   "implementation": "oracle multiversion ordered map (std::map per key-range "
+                                     "partition, one partition per host thread)"},
+        "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    args = parse_args()
+    dist = Dist()
+    if args.impl == "reference":
+        out = run_reference(args, dist)
+        if out is not None:
+            print(json.dumps(out), flush=True)
+        return
+    out, cpu_inputs = run_ours(args, dist)
+    if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
+        init, vals, step = cpu_inputs
+        cores, build_s, times, ops = cpu_oracle_time(init, vals, [step], args.cpu_sample_ops)
+        out["cpu_baseline"] = {
+            "value": round(ops[0] / times[0] / 1e6, 3), "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{ops[0]} ops (first batches of one step) on the 40M-key oracle map, "
+                      f"{cores} threads; build {build_s:.1f} s untimed"}
+    if dist.rank == 0:
+        print(json.dumps(out), flush=True)
+    dist.close()
+
+
+if __name__ == "__main__":
+    main()

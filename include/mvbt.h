@@ -230,6 +230,12 @@ int mvbt_batch_run(mvbt_batch_plan* plan, uint32_t num_batches, const uint64_t* 
                    const uint64_t* out_off, const uint32_t* range_cap, uint32_t* result,
                    mvbt_pair* range_out, int mode, void* stream);
 
+/* enable = 1 records CUDA events around the persistent kernel of each MVBT_BATCH_PERSISTENT run
+ * (up to 64 runs are kept); mvbt_batch_plan_kernel_times waits for them, writes the kernel times
+ * in ms of the runs since the last call (oldest first, at most max) and their number to *n. */
+int mvbt_batch_plan_timing(mvbt_batch_plan* plan, int enable);
+int mvbt_batch_plan_kernel_times(mvbt_batch_plan* plan, float* ms, uint32_t max, uint32_t* n);
+
 /* Tree kind, tile width and device of a handle. */
 int mvbt_get_info(mvbt_tree* tree, int* kind, int* tile_width, int* device);
 

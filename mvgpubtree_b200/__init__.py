@@ -86,6 +86,9 @@ _sig("mvbt_get_info", ctypes.c_int, _vp, ctypes.POINTER(ctypes.c_int), ctypes.PO
 _sig("mvbt_batch_plan_create", ctypes.c_int, _vp, _u64, _u32, ctypes.POINTER(_vp))
 _sig("mvbt_batch_plan_destroy", ctypes.c_int, _vp)
 _sig("mvbt_batch_run", ctypes.c_int, _vp, _u32, _vp, _P, _P, _P, _P, _P, _P, _P, ctypes.c_int, _vp)
+_sig("mvbt_batch_plan_timing", ctypes.c_int, _vp, ctypes.c_int)
+_sig("mvbt_batch_plan_kernel_times", ctypes.c_int, _vp, ctypes.POINTER(ctypes.c_float), _u32,
+     ctypes.POINTER(_u32))
 _sig("mvbt_last_error", ctypes.c_char_p)
 _sig("mvbt_status_string", ctypes.c_char_p, ctypes.c_int)
 
@@ -339,6 +342,18 @@ class BatchPlan:
                                   _ptr(out_off, 8, "out_off"), _ptr(range_cap, name="range_cap"),
                                   _ptr(result, name="result"), _ptr(range_out, 8, "range_out"),
                                   int(mode), _stream(stream)), "batch_run")
+
+    def enable_timing(self, on: bool = True) -> None:
+        """CUDA events around the persistent kernel of each BATCH_PERSISTENT run."""
+        _check(lib.mvbt_batch_plan_timing(self._h, int(bool(on))), "batch_plan_timing")
+
+    def kernel_times(self) -> list:
+        """Persistent-kernel times (ms) of the runs since the last call (waits for them)."""
+        buf = (ctypes.c_float * 64)()
+        n = _u32(0)
+        _check(lib.mvbt_batch_plan_kernel_times(self._h, buf, 64, ctypes.byref(n)),
+               "batch_plan_kernel_times")
+        return [float(buf[i]) for i in range(n.value)]
 
     def close(self):
         if getattr(self, "_h", None):

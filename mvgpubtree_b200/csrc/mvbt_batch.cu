@@ -41,6 +41,11 @@ struct mvbt_batch_plan {
   cudaGraphExec_t graph;
   bool have_graph;
   const void* graph_key[8];
+  // optional CUDA events around the persistent kernel (PERSISTENT mode), a ring of pairs
+  static constexpr int kTimed = 64;
+  bool timing;
+  uint32_t timed_runs;
+  cudaEvent_t ev_begin[kTimed], ev_end[kTimed];
 };
 
 namespace {
@@ -196,10 +201,16 @@ int enqueue_persistent(mvbt_batch_plan* p, const launch_ctx& c, const batch_view
   sc.cursor      = p->d_cursor;
   sc.params      = p->d_params;
   sc.chunk       = 16;
+  const int slot = (int)(p->timed_runs % mvbt_batch_plan::kTimed);
+  if (p->timing) cudaEventRecord(p->ev_begin[slot], s);
   if (c.W == 8) {
     k_batched<8><<<occupancy_grid(c, k_batched<8>), c.block, 0, s>>>(c.view, B, sc);
   } else {
     k_batched<16><<<occupancy_grid(c, k_batched<16>), c.block, 0, s>>>(c.view, B, sc);
+  }
+  if (p->timing) {
+    cudaEventRecord(p->ev_end[slot], s);
+    ++p->timed_runs;
   }
   k_batch_end<<<1, 32, 0, s>>>(c.ctl, p->d_params);
   cudaError_t e = cudaGetLastError();
@@ -253,6 +264,7 @@ int mvbt_batch_plan_destroy(mvbt_batch_plan* p) {
   cudaFree(p->d_cursor);
   cudaFreeHost(p->h_batch_off);
   cudaFreeHost(p->h_params);
+  mvbt_batch_plan_timing(p, 0);
   delete p;
   return MVBT_OK;
 }
@@ -312,6 +324,7 @@ int mvbt_batch_run(mvbt_batch_plan* p, uint32_t num_batches, const uint64_t* bat
   p->h_params[1] = 0;
 
   if (mode == MVBT_BATCH_PERSISTENT) return enqueue_persistent(p, c, B, s);
+  if (p->timing) return fail(MVBT_ERR_BAD_ARG, "kernel timing is available in MVBT_BATCH_PERSISTENT mode");
   if (mode != MVBT_BATCH_GRAPH) return fail(MVBT_ERR_BAD_ARG, "unknown batch mode");
 
   const void* key_now[8] = {type, key, arg, out_off, range_cap, result, range_out, stream};
@@ -336,6 +349,40 @@ int mvbt_batch_run(mvbt_batch_plan* p, uint32_t num_batches, const uint64_t* bat
     std::memcpy(p->graph_key, key_now, sizeof(key_now));
   }
   MVBT_TRY(cudaGraphLaunch(p->graph, s));
+  return MVBT_OK;
+}
+
+int mvbt_batch_plan_timing(mvbt_batch_plan* p, int enable) {
+  if (!p) return fail(MVBT_ERR_BAD_ARG, "null plan");
+  if (enable && !p->timing) {
+    for (int i = 0; i < mvbt_batch_plan::kTimed; ++i) {
+      MVBT_TRY(cudaEventCreate(&p->ev_begin[i]));
+      MVBT_TRY(cudaEventCreate(&p->ev_end[i]));
+    }
+    p->timing = true;
+  } else if (!enable && p->timing) {
+    for (int i = 0; i < mvbt_batch_plan::kTimed; ++i) {
+      cudaEventDestroy(p->ev_begin[i]);
+      cudaEventDestroy(p->ev_end[i]);
+    }
+    p->timing = false;
+  }
+  p->timed_runs = 0;
+  return MVBT_OK;
+}
+
+int mvbt_batch_plan_kernel_times(mvbt_batch_plan* p, float* ms, uint32_t max, uint32_t* n) {
+  if (!p || !ms || !n || !p->timing) return fail(MVBT_ERR_BAD_ARG, "timing is not enabled");
+  const uint32_t have = std::min<uint32_t>(p->timed_runs, mvbt_batch_plan::kTimed);
+  const uint32_t first = p->timed_runs - have;
+  uint32_t k = 0;
+  for (uint32_t r = first; r < p->timed_runs && k < max; ++r, ++k) {
+    const int slot = (int)(r % mvbt_batch_plan::kTimed);
+    MVBT_TRY(cudaEventSynchronize(p->ev_end[slot]));
+    MVBT_TRY(cudaEventElapsedTime(&ms[k], p->ev_begin[slot], p->ev_end[slot]));
+  }
+  *n            = k;
+  p->timed_runs = 0;
   return MVBT_OK;
 }
 
