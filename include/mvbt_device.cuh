@@ -34,8 +34,10 @@
 //     moves right under lock coupling, and applies its change; a full node splits into itself
 //     and a new right sibling (right written first, then left, each followed by a fence), then
 //     the writer releases the node and inserts the separator into the parent recorded on its
-//     way down (moving right there as needed); the root keeps index 0 and grows by copying its
-//     halves into two new children;
+//     way down (moving right there as needed); node 0 is a fixed anchor whose single entry points
+//     at the top of the tree, and the tree grows by building a new top node and re-pointing the
+//     anchor, so no node ever changes its level or role (a reader that sees a mix of two
+//     versions of a node still follows a valid route);
 //   * versioning (versioned trees): a writer in epoch E that first touches a node whose ts < E
 //     copies it to a fresh node O, publishes the header {ts = E, older = O} before changing the
 //     data, and nodes created by splits in epoch E point to the same O. A reader at snapshot S
@@ -100,7 +102,8 @@ constexpr uint32_t kLatest    = 0xFFFFFFFFu;  // read the newest version
 constexpr uint32_t kNone      = 0x0FFFFFFFu;  // "no node" in 28-bit index fields
 constexpr uint32_t kIndexMask = 0x0FFFFFFFu;
 constexpr uint32_t kLockBit   = 0x80000000u;
-constexpr uint32_t kRoot      = 0;
+constexpr uint32_t kAnchor    = 0;  // fixed entry node: one entry {0 -> top}, level = top + 1
+constexpr uint32_t kFirstLeaf = 1;  // the initial leaf (holds the tombstone {0, 0})
 constexpr int kMaxLevels      = 16;
 constexpr int kMaxSmSlots     = 256;
 constexpr uint32_t kMaxSteps  = 1u << 16;  // node visits per operation before giving up
@@ -136,22 +139,30 @@ struct control_block {
 #define MVBT_HD __host__ __device__ __forceinline__
 #endif
 
-// Word t (0..31) of the initial root: a leaf holding the tombstone {0, 0}, empty pairs,
-// high key 0xFFFFFFFF, no sibling, ts 0, no older version, level 0.
-MVBT_HD uint32_t initial_root_word(int t) {
-  if (t == 0 || t == 1) return 0u;
-  if (t < 28) return kEmptyKey;
-  if (t == 28) return kEmptyKey;  // high key
-  if (t == 29) return kNone;      // link
-  if (t == 30) return 0u;         // ts
-  return kNone;                   // older | level 0
+// Word t (0..63) of the initial tree. Node 0 is the anchor: an interior node whose only entry
+// {0 -> 1} points at the top of the tree, level 1. Node 1 is a leaf holding the tombstone {0, 0}.
+// Both have high key 0xFFFFFFFF, no sibling, ts 0 and no older version. The anchor's single
+// entry is the only pointer that changes when the tree grows, and no node ever changes level, so
+// a reader that sees a mix of two versions of any node still finds a valid route.
+MVBT_HD uint32_t initial_tree_word(int t) {
+  const int node = t >> 5, w = t & 31;
+  if (w < 28) {
+    if (w == 0) return 0u;                           // first key: 0
+    if (w == 1) return node == 0 ? kFirstLeaf : 0u;  // anchor -> leaf 1; tombstone value 0
+    return kEmptyKey;
+  }
+  if (w == 28) return kEmptyKey;                     // high key
+  if (w == 29) return kNone;                         // link
+  if (w == 30) return 0u;                            // ts
+  return (node == 0 ? (1u << 28) : 0u) | kNone;      // level | no older version
 }
+constexpr int kInitialNodes = 2;
 
 MVBT_HD void init_control(control_block& c, uint32_t capacity, uint32_t chunk, uint32_t spin_limit,
                           uint32_t wait_ns) {
   c.epoch         = 0;
   c.error         = 0;
-  c.bump          = 1;  // node 0 is the root
+  c.bump          = kInitialNodes;  // nodes 0 (anchor) and 1 (first leaf)
   c.capacity      = capacity;
   c.chunk         = chunk;
   c.spin_limit    = spin_limit;
@@ -596,9 +607,18 @@ struct device_tree {
   // ---- versioning ----
   // Makes the version visible to older snapshots immutable before node idx (locked, content n)
   // is changed in epoch E: copies n to a fresh node and publishes {ts = E, older = copy}.
+  // On a plain tree the ts word counts modifications instead: it is bumped and published before
+  // the data changes, so a concurrent reader that re-reads it after a fence sees any change.
   template <int W, class Tile>
   MVBT_DEV bool prepare_write(uint32_t idx, node_regs<W>& n, header& h, uint32_t E, const Tile& t) const {
-    if (!versioned || h.ts == E) return true;
+    if (!versioned) {
+      h.ts += 1;
+      set_header<W>(n, h, t);
+      store_header<W>(idx, n, t);
+      __threadfence();
+      return true;
+    }
+    if (h.ts == E) return true;
     uint32_t copy = alloc(t);
     if (copy == kNone) return false;
     node_regs<W> c = n;
@@ -641,6 +661,16 @@ struct device_tree {
   // ts <= snapshot re-reads the header after a fence. A writer publishes {ts = E, older = copy}
   // before it changes the data, so if any lane saw changed data the re-read shows ts > snapshot:
   // the reader then returns the index of the immutable copy (else kNone: the data is consistent).
+  // The plain-tree counterpart: true if the modification count of leaf idx is no longer `seen`.
+  template <class Tile>
+  MVBT_DEV bool leaf_changed(uint32_t idx, uint32_t seen, const Tile& t) const {
+    __threadfence();
+    t.sync();
+    uint32_t now = 0;
+    if (t.thread_rank() == 0) now = ld_relaxed_u32(node_ptr(idx) + 30);
+    return t.shfl(now, 0) != seen;
+  }
+
   template <class Tile>
   MVBT_DEV uint32_t recheck_version(uint32_t idx, uint32_t ts, const Tile& t) const {
     __threadfence();
@@ -660,7 +690,7 @@ struct device_tree {
   MVBT_DEV uint32_t cooperative_find(uint32_t key, const Tile& t, uint32_t ts = kLatest,
                                      bool concurrent = false) const {
     const bool snap = versioned && ts != kLatest;
-    uint32_t idx    = kRoot;
+    uint32_t idx    = kAnchor;
     bool via_older  = false;  // idx was reached through an older-version pointer
     node_regs<W> n;
     for (uint32_t step = 0; step < kMaxSteps; ++step) {
@@ -682,6 +712,8 @@ struct device_tree {
             via_older = true;
             continue;
           }
+        } else if (!versioned && concurrent && leaf_changed(idx, h.ts, t)) {
+          continue;  // a writer changed the leaf while it was read: read it again
         }
         return leaf_value<W>(n, key, t);
       }
@@ -701,7 +733,7 @@ struct device_tree {
     constexpr int P = 16 / W;
     if (hi <= lo) return 0;
     const bool snap = versioned && ts != kLatest;
-    uint32_t idx    = kRoot;
+    uint32_t idx    = kAnchor;
     bool via_older  = false;
     node_regs<W> n;
     header h;
@@ -729,6 +761,8 @@ struct device_tree {
             via_older = true;
             continue;
           }
+        } else if (!versioned && concurrent && leaf_changed(idx, h.ts, t)) {
+          continue;
         }
         break;
       }
@@ -782,6 +816,8 @@ struct device_tree {
             via_older = true;
             continue;
           }
+        } else if (!versioned && concurrent && leaf_changed(idx, h.ts, t)) {
+          continue;
         }
         settled = true;
       }
@@ -801,7 +837,7 @@ struct device_tree {
   template <int W, class Tile>
   MVBT_DEV uint32_t descend_for_write(uint32_t key, uint32_t& path0, uint32_t& path1,
                                       uint32_t& top_level, const Tile& t) const {
-    uint32_t idx = kRoot;
+    uint32_t idx = kAnchor;
     node_regs<W> n;
     top_level = 0;
     bool first = true;
@@ -843,8 +879,8 @@ struct device_tree {
       if (h.level() != level) {
         unlock(idx, t);
         if (h.level() < level) {
-          // The root is the only node whose level changes, and it only grows; a lower level
-          // here means the caller's route is broken.
+          // Only the anchor (node 0) changes level, and only upwards when the tree grows; a
+          // lower level here means the caller's route is broken.
           if (t.thread_rank() == 0) set_error(kErrCorrupt);
           return kNone;
         }
@@ -873,6 +909,11 @@ struct device_tree {
         idx = sib;
         load<W>(idx, n, true, t);
         h = get_header<W>(n, t);
+        if (h.level() != level) {  // a right link always stays on its level
+          unlock(idx, t);
+          if (t.thread_rank() == 0) set_error(kErrCorrupt);
+          return kNone;
+        }
         if (++hops > kMaxSteps) {
           unlock(idx, t);
           if (t.thread_rank() == 0) set_error(kErrStepLimit);
@@ -886,50 +927,15 @@ struct device_tree {
   }
 
   // Splits locked node idx (content n, header h, already prepared for epoch E) while inserting
-  // {key, val}. The left half stays in idx, the right half goes to a new node. For the root the
-  // two halves go to two new children and the root becomes their parent. Outputs the separator
-  // and new right node to insert into the parent (sep_child = kNone when the root was split).
-  // The lock on idx is released.
+  // {key, val}: the left half stays in idx, the right half goes to a new node written first.
+  // Outputs the separator and the new node for the parent; releases the lock on idx. New nodes
+  // of epoch E point at the version of idx older snapshots read, so such a reader that reaches
+  // one continues from a node that covers its key.
   template <int W, class Tile>
   MVBT_DEV bool split_insert(uint32_t idx, node_regs<W>& n, header& h, uint32_t key, uint32_t val,
                              uint32_t E, uint32_t& sep_key, uint32_t& sep_child, const Tile& t) const {
-    const int pos = count_less<W>(n, key, t);
+    const int pos     = count_less<W>(n, key, t);
     const uint32_t ts = versioned ? E : 0u;
-    if (idx == kRoot) {
-      uint32_t a = alloc(t);
-      uint32_t b = (a == kNone) ? kNone : alloc(t);
-      if (b == kNone) {
-        unlock(idx, t);
-        return false;
-      }
-      node_regs<W> left, right;
-      build_from_merged<W>(n, pos, key, val, 0, kSplitLeft, left, t);
-      build_from_merged<W>(n, pos, key, val, kSplitLeft, kDataPairs + 1 - kSplitLeft, right, t);
-      uint32_t rmin = t.shfl(right.k[0], 0);
-      const uint32_t older = versioned ? h.older() : kNone;
-      header hr{kEmptyKey, kNone, ts, (h.level() << 28) | older};
-      header hl{rmin, b, ts, (h.level() << 28) | older};
-      set_header<W>(right, hr, t);
-      set_header<W>(left, hl, t);
-      store<W>(b, right, t);
-      store<W>(a, left, t);
-      __threadfence();
-      // new root content: {0, a}, {rmin, b}
-      node_regs<W> root;
-#pragma unroll
-      for (int j = 0; j < 16 / W; ++j) {
-        int q     = pair_index<W>(t, j);
-        root.k[j] = q == 0 ? 0u : (q == 1 ? rmin : kEmptyKey);
-        root.v[j] = q == 0 ? a : (q == 1 ? b : kEmptyKey);
-      }
-      header hroot{kEmptyKey, kNone | kLockBit, versioned ? E : h.ts, ((h.level() + 1) << 28) | older};
-      set_header<W>(root, hroot, t);
-      store<W>(idx, root, t);
-      if (t.thread_rank() == 0) atomicAdd(&ctl->stat_split, 1ull);
-      unlock(idx, t);
-      sep_child = kNone;
-      return true;
-    }
     uint32_t r = alloc(t);
     if (r == kNone) {
       unlock(idx, t);
@@ -950,6 +956,41 @@ struct device_tree {
     unlock(idx, t);
     sep_key   = rmin;
     sep_child = r;
+    return true;
+  }
+
+  // The split node was the top: build a new top {0 -> old top, sep -> new node} one level up and
+  // point the (locked, prepared) anchor at it. Releases the anchor.
+  template <int W, class Tile>
+  MVBT_DEV bool grow(node_regs<W>& n, header& h, uint32_t sep_key, uint32_t sep_child, uint32_t E,
+                     const Tile& t) const {
+    const uint32_t old_top = t.shfl(n.v[0], 0);
+    const uint32_t top     = alloc(t);
+    if (top == kNone) {
+      unlock(kAnchor, t);
+      return false;
+    }
+    const uint32_t lvl   = h.level();  // level of the new top
+    const uint32_t older = versioned ? h.older() : kNone;
+    node_regs<W> x;
+#pragma unroll
+    for (int j = 0; j < 16 / W; ++j) {
+      const int q = pair_index<W>(t, j);
+      x.k[j]      = q == 0 ? 0u : (q == 1 ? sep_key : kEmptyKey);
+      x.v[j]      = q == 0 ? old_top : (q == 1 ? sep_child : kEmptyKey);
+    }
+    header hx{kEmptyKey, kNone, versioned ? E : 0u, (lvl << 28) | older};
+    set_header<W>(x, hx, t);
+    store<W>(top, x, t);
+    __threadfence();
+#pragma unroll
+    for (int j = 0; j < 16 / W; ++j)
+      if (pair_index<W>(t, j) == 0) n.v[j] = top;
+    h.ol = ((lvl + 1) << 28) | (h.ol & kIndexMask);
+    set_header<W>(n, h, t);
+    store<W>(kAnchor, n, t);
+    if (t.thread_rank() == 0) atomicAdd(&ctl->stat_split, 1ull);
+    unlock(kAnchor, t);
     return true;
   }
 
@@ -1000,9 +1041,9 @@ struct device_tree {
         uint32_t start;
         if (level <= top) {
           start = (level < (uint32_t)W) ? t.shfl(path0, level) : t.shfl(path1, level - W);
-          if (start == kNone) start = kRoot;
+          if (start == kNone) start = kAnchor;
         } else {
-          start = kRoot;
+          start = kAnchor;
         }
         if (level >= (uint32_t)kMaxLevels) {
           if (t.thread_rank() == 0) set_error(kErrCorrupt);
@@ -1014,6 +1055,7 @@ struct device_tree {
           unlock(p, t);
           return false;
         }
+        if (p == kAnchor) return grow<W>(n, h, sep_key, sep_child, E, t);
         nvalid = count_valid<W>(n, t);
         if (nvalid < kDataPairs) {
           int ipos = count_less<W>(n, sep_key, t);

@@ -68,7 +68,7 @@ inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s
 // ----------------------------------------------------------------------------------------------
 __global__ void k_init(uint32_t* pool, control_block* c, uint32_t capacity, uint32_t chunk,
                        uint32_t spin_limit, uint32_t wait_ns) {
-  if (threadIdx.x < 32) pool[threadIdx.x] = mvbt::initial_root_word(threadIdx.x);
+  for (int i = threadIdx.x; i < 32 * mvbt::kInitialNodes; i += blockDim.x) pool[i] = mvbt::initial_tree_word(i);
   if (threadIdx.x == 0) mvbt::init_control(*c, capacity, chunk, spin_limit, wait_ns);
 }
 

@@ -67,8 +67,8 @@ extern "C" int mvbt_validate_image_detail(const uint32_t* img, uint64_t nn, int 
     rep->violations = 1;
     return MVBT_ERR_CORRUPT;
   }
-  const int top  = (int)node(root).level();
-  rep->height    = (uint32_t)top + 1;
+  const int top  = (int)node(root).level();  // node 0 is the anchor, one level above the top
+  rep->height    = (uint32_t)top;
   uint32_t first = 0;  // slot index of the leftmost node of the level
   std::vector<uint32_t> child_slots;
   for (int level = top; level >= 0; --level) {
@@ -164,6 +164,7 @@ extern "C" int mvbt_validate_image_detail(const uint32_t* img, uint64_t nn, int 
       first = node(v).val(0);
     }
   }
+  if (rep->interior) --rep->interior;  // the anchor is not a tree node
   rep->violations = violations;
   if (detail && detail_len) {
     size_t c = std::min<size_t>(log.size(), detail_len - 1);

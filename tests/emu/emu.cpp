@@ -93,7 +93,7 @@ void* emu_create(int versioned, uint32_t capacity, uint32_t spin_limit, uint32_t
   t->capacity  = capacity;
   t->versioned = versioned;
   t->pool.assign((size_t)capacity * 32, 0xA5A5A5A5u);  // garbage, as fresh cudaMalloc memory
-  for (int i = 0; i < 32; ++i) t->pool[i] = mvbt::initial_root_word(i);
+  for (int i = 0; i < 32 * mvbt::kInitialNodes; ++i) t->pool[i] = mvbt::initial_tree_word(i);
   mvbt::init_control(t->ctl, capacity, chunk ? chunk : 8, spin_limit ? spin_limit : (1u << 20),
                      200u * 1000u * 1000u);
   return t;
