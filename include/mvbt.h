@@ -190,6 +190,12 @@ int mvbt_validate_image_detail(const uint32_t* image, uint64_t nodes, int versio
  * mvbt_validate_image or stored as a dump of the tree. */
 int mvbt_copy_pool(mvbt_tree* tree, void* dst, uint64_t max_nodes, uint64_t* nodes);
 
+/* Device counters (synchronises the device): out[0] versions copied, [1] node splits, [2] longest
+ * locked move-right walk, [3] longest unlocked writer descent, [4] write epoch, [5] error bits,
+ * [6..21] errors per raising site, [22] locked approaches restarted unlocked. Writes min(n, 23)
+ * values. */
+int mvbt_stats(mvbt_tree* tree, uint64_t* out, uint32_t n);
+
 /* Device view for user kernels calling the cooperative_* device API. */
 int mvbt_get_device_view(mvbt_tree* tree, mvbt_device_view* out);
 

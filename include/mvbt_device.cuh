@@ -73,6 +73,12 @@ template <class T, class U>
 inline T atomicAdd(T* p, U v) { return __atomic_fetch_add(p, (T)v, __ATOMIC_SEQ_CST); }
 template <class T, class U>
 inline T atomicExch(T* p, U v) { return __atomic_exchange_n(p, (T)v, __ATOMIC_SEQ_CST); }
+template <class T, class U>
+inline T atomicMax(T* p, U v) {
+  T cur = __atomic_load_n(p, __ATOMIC_RELAXED);
+  while (cur < (T)v && !__atomic_compare_exchange_n(p, &cur, (T)v, false, __ATOMIC_SEQ_CST, __ATOMIC_RELAXED)) {}
+  return cur;
+}
 namespace mvbt {
 namespace emu {
 inline thread_local uint32_t sm = 0;  // emulated SM id of the calling lane
@@ -107,6 +113,8 @@ constexpr uint32_t kFirstLeaf = 1;  // the initial leaf (holds the tombstone {0,
 constexpr int kMaxLevels      = 16;
 constexpr int kMaxSmSlots     = 256;
 constexpr uint32_t kMaxSteps  = 1u << 16;  // node visits per operation before giving up
+constexpr uint32_t kCoupledHops  = 4;       // right moves taken while holding a lock
+constexpr uint32_t kChaseRestart = 16;      // unlocked right moves before restarting at the anchor
 
 // Sticky error bits in control_block::error.
 enum : uint32_t {
@@ -128,8 +136,10 @@ struct control_block {
   uint32_t reserved;
   unsigned long long stat_cow;    // copy-on-write versions created
   unsigned long long stat_split;  // node splits
-  unsigned long long stat_restart;
-  unsigned long long stat_reserved;
+  unsigned long long stat_max_hops;   // longest move-right walk under locks
+  unsigned long long stat_max_steps;  // longest unlocked descent of a writer (node visits)
+  unsigned long long stat_restarts;   // locked approaches abandoned for an unlocked re-approach
+  uint32_t err_site[16];              // errors per raising site (diagnostics)
   unsigned long long sm_pool[kMaxSmSlots];  // per-SM chunk cursor: (base << 32) | used
 };
 
@@ -170,8 +180,10 @@ MVBT_HD void init_control(control_block& c, uint32_t capacity, uint32_t chunk, u
   c.reserved      = 0;
   c.stat_cow      = 0;
   c.stat_split    = 0;
-  c.stat_restart  = 0;
-  c.stat_reserved = 0;
+  c.stat_max_hops  = 0;
+  c.stat_restarts  = 0;
+  c.stat_max_steps = 0;
+  for (int i = 0; i < 16; ++i) c.err_site[i] = 0;
   // used == chunk: the first allocation on each SM refills its chunk from the bump pointer
   for (int i = 0; i < kMaxSmSlots; ++i) c.sm_pool[i] = chunk;
 }
@@ -501,7 +513,7 @@ struct device_tree {
   template <class Tile>
   MVBT_DEV bool valid(uint32_t idx, const Tile& t) const {
     if (idx < capacity) return true;
-    if (t.thread_rank() == 0) set_error(kErrCorrupt);
+    if (t.thread_rank() == 0) set_error(kErrCorrupt, 1);
     return false;
   }
 
@@ -521,7 +533,11 @@ struct device_tree {
     if (r == L::kLinkLane || r == L::kVerLane) st_lane<W>(node_ptr(idx) + r * (32 / W), n);
   }
 
-  MVBT_DEV void set_error(uint32_t bits) const { atomicOr(&ctl->error, bits); }
+  // Records error bits and counts the site that raised them (control_block::err_site).
+  MVBT_DEV void set_error(uint32_t bits, uint32_t site = 0) const {
+    atomicOr(&ctl->error, bits);
+    atomicAdd(&ctl->err_site[site & 15], 1u);
+  }
   MVBT_DEV uint32_t current_epoch() const { return ld_relaxed_u32(&ctl->epoch); }
 
   // ---- allocation: per-SM chunks carved from a global bump pointer ----
@@ -540,6 +556,7 @@ struct device_tree {
         uint32_t nb = atomicAdd(&c->bump, C);
         if ((unsigned long long)nb + C > c->capacity) {
           atomicOr(&c->error, kErrPoolExhausted);
+          atomicAdd(&c->err_site[15], 1u);
           return kNone;
         }
         atomicExch(slot, ((unsigned long long)nb << 32) | 1ull);
@@ -556,6 +573,7 @@ struct device_tree {
       if (global_ns() - t0 > c->wait_ns) break;
     }
     atomicOr(&c->error, kErrSpinLimit);
+    atomicAdd(&c->err_site[0], 1u);
     return kNone;
   }
   template <class Tile>
@@ -594,7 +612,7 @@ struct device_tree {
       }
       if (global_ns() - t0 > lns) break;
     }
-    if (t.thread_rank() == 0) set_error(kErrSpinLimit);
+    if (t.thread_rank() == 0) set_error(kErrSpinLimit, 2);
     return false;
   }
   template <class Tile>
@@ -645,7 +663,7 @@ struct device_tree {
     while (h.ts > ts) {
       uint32_t older = h.older();
       if (older == kNone || ++hops > kMaxSteps) {
-        if (t.thread_rank() == 0) set_error(kErrCorrupt);
+        if (t.thread_rank() == 0) set_error(kErrCorrupt, 3);
         return false;
       }
       idx = older;
@@ -719,7 +737,7 @@ struct device_tree {
       }
       idx = child_for<W>(n, key, t);
     }
-    if (t.thread_rank() == 0) set_error(kErrStepLimit);
+    if (t.thread_rank() == 0) set_error(kErrStepLimit, 4);
     return kNotFound;
   }
 
@@ -740,7 +758,7 @@ struct device_tree {
     // descend to the leaf that holds lo and settle on a consistent version of it
     for (uint32_t step = 0;; ++step) {
       if (step >= kMaxSteps) {
-        if (t.thread_rank() == 0) set_error(kErrStepLimit);
+        if (t.thread_rank() == 0) set_error(kErrStepLimit, 5);
         return 0;
       }
       if (!valid(idx, t)) return 0;
@@ -796,7 +814,7 @@ struct device_tree {
       count += inr;
       if (!(hi > h.high && h.sibling() != kNone)) break;
       if (leaves >= capacity) {
-        if (t.thread_rank() == 0) set_error(kErrStepLimit);
+        if (t.thread_rank() == 0) set_error(kErrStepLimit, 6);
         break;
       }
       // next leaf: load, resolve the snapshot version, validate before its data is used
@@ -822,7 +840,7 @@ struct device_tree {
         settled = true;
       }
       if (!settled) {
-        if (t.thread_rank() == 0) set_error(kErrStepLimit);
+        if (t.thread_rank() == 0) set_error(kErrStepLimit, 7);
         return count;
       }
     }
@@ -854,7 +872,10 @@ struct device_tree {
         continue;
       }
       uint32_t lvl = h.level();
-      if (lvl == 0) return idx;
+      if (lvl == 0) {
+        if (step > 16 && t.thread_rank() == 0) atomicMax(&ctl->stat_max_steps, (unsigned long long)step);
+        return idx;
+      }
       if (lvl < (uint32_t)W) {
         if (t.thread_rank() == (int)lvl) path0 = idx;
       } else {
@@ -862,44 +883,63 @@ struct device_tree {
       }
       idx = child_for<W>(n, key, t);
     }
-    if (t.thread_rank() == 0) set_error(kErrStepLimit);
+    if (t.thread_rank() == 0) set_error(kErrStepLimit, 8);
     return kNone;
   }
 
-  // Locks the node at `level` that covers key, starting from `idx` (a node at level >= level
-  // on the right path, typically the recorded parent). Returns the locked index, with n/h
+  // Unlocked approach to the node at `level` whose range covers key, starting from idx (a node
+  // at `level` or above on key's route): walks down along key and right along links. A long
+  // chase to the right means the start is stale (many splits since it was read), so the walk
+  // restarts from the anchor, which reaches the key in about height steps. Returns the index
+  // with n/h loaded, or kNone on failure.
+  template <int W, class Tile>
+  MVBT_DEV uint32_t seek(uint32_t idx, uint32_t level, uint32_t key, node_regs<W>& n, header& h,
+                         const Tile& t) const {
+    uint32_t chase = 0;
+    for (uint32_t step = 0; step < kMaxSteps; ++step) {
+      if (!valid(idx, t)) return kNone;
+      load<W>(idx, n, true, t);
+      h = get_header<W>(n, t);
+      if (key >= h.high && h.sibling() != kNone) {
+        if (++chase > kChaseRestart) {
+          idx   = kAnchor;
+          chase = 0;
+        } else {
+          idx = h.sibling();
+        }
+        continue;
+      }
+      if (h.level() == level) return idx;
+      if (h.level() < level) {
+        if (t.thread_rank() == 0) set_error(kErrCorrupt, 9);
+        return kNone;
+      }
+      idx   = child_for<W>(n, key, t);
+      chase = 0;
+    }
+    if (t.thread_rank() == 0) set_error(kErrStepLimit, 12);
+    return kNone;
+  }
+
+  // Locks the node at `level` that covers key, starting from idx (the node recorded on the way
+  // down, or the anchor). Only a few lock-coupled hops to the right are taken while holding a
+  // lock; a node further right is re-approached unlocked. Returns the locked index with n/h
   // loaded; kNone on failure.
   template <int W, class Tile>
   MVBT_DEV uint32_t lock_covering(uint32_t idx, uint32_t level, uint32_t key, node_regs<W>& n,
                                   header& h, const Tile& t) const {
-    for (uint32_t step = 0; step < kMaxSteps; ++step) {
+    for (uint32_t attempt = 0; attempt < kMaxSteps; ++attempt) {
+      idx = seek<W>(idx, level, key, n, h, t);
+      if (idx == kNone) return kNone;
       if (!lock(idx, t)) return kNone;
       load<W>(idx, n, true, t);
       h = get_header<W>(n, t);
-      if (h.level() != level) {
+      if (h.level() != level) {  // only the anchor changes level: re-approach from it
         unlock(idx, t);
-        if (h.level() < level) {
-          // Only the anchor (node 0) changes level, and only upwards when the tree grows; a
-          // lower level here means the caller's route is broken.
-          if (t.thread_rank() == 0) set_error(kErrCorrupt);
-          return kNone;
-        }
-        // The tree grew above this node: walk down (unlocked) to `level` along key.
-        for (uint32_t s2 = 0; s2 < kMaxSteps && h.level() > level; ++s2) {
-          if (key >= h.high && h.sibling() != kNone) {
-            idx = h.sibling();
-          } else {
-            idx = child_for<W>(n, key, t);
-          }
-          if (!valid(idx, t)) return kNone;
-          load<W>(idx, n, true, t);
-          h = get_header<W>(n, t);
-        }
         continue;
       }
-      // Move right under lock coupling while key belongs further right.
       uint32_t hops = 0;
-      while (key >= h.high && h.sibling() != kNone) {
+      while (key >= h.high && h.sibling() != kNone && hops < kCoupledHops) {
         uint32_t sib = h.sibling();
         if (!lock(sib, t)) {
           unlock(idx, t);
@@ -909,20 +949,19 @@ struct device_tree {
         idx = sib;
         load<W>(idx, n, true, t);
         h = get_header<W>(n, t);
+        ++hops;
         if (h.level() != level) {  // a right link always stays on its level
           unlock(idx, t);
-          if (t.thread_rank() == 0) set_error(kErrCorrupt);
-          return kNone;
-        }
-        if (++hops > kMaxSteps) {
-          unlock(idx, t);
-          if (t.thread_rank() == 0) set_error(kErrStepLimit);
+          if (t.thread_rank() == 0) set_error(kErrCorrupt, 10);
           return kNone;
         }
       }
-      return idx;
+      if (hops > 2 && t.thread_rank() == 0) atomicMax(&ctl->stat_max_hops, (unsigned long long)hops);
+      if (!(key >= h.high && h.sibling() != kNone)) return idx;
+      unlock(idx, t);  // still far to the left: approach again without holding locks
+      if (t.thread_rank() == 0) atomicAdd(&ctl->stat_restarts, 1ull);
     }
-    if (t.thread_rank() == 0) set_error(kErrStepLimit);
+    if (t.thread_rank() == 0) set_error(kErrStepLimit, 11);
     return kNone;
   }
 
@@ -1046,7 +1085,7 @@ struct device_tree {
           start = kAnchor;
         }
         if (level >= (uint32_t)kMaxLevels) {
-          if (t.thread_rank() == 0) set_error(kErrCorrupt);
+          if (t.thread_rank() == 0) set_error(kErrCorrupt, 13);
           return false;
         }
         uint32_t p = lock_covering<W>(start, level, sep_key, n, h, t);
@@ -1215,7 +1254,7 @@ MVBT_DEV void batched_worker(const device_tree& T, const batch_view& B, const ba
             __nanosleep(w < 16 ? 64 : 256);
           }
           if (!ok) {
-            if (t.thread_rank() == 0) T.set_error(kErrSpinLimit);
+            if (t.thread_rank() == 0) T.set_error(kErrSpinLimit, 14);
           }
           __threadfence();
         }

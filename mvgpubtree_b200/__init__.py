@@ -89,6 +89,7 @@ _sig("mvbt_batch_run", ctypes.c_int, _vp, _u32, _vp, _P, _P, _P, _P, _P, _P, _P,
 _sig("mvbt_batch_plan_timing", ctypes.c_int, _vp, ctypes.c_int)
 _sig("mvbt_batch_plan_kernel_times", ctypes.c_int, _vp, ctypes.POINTER(ctypes.c_float), _u32,
      ctypes.POINTER(_u32))
+_sig("mvbt_stats", ctypes.c_int, _vp, ctypes.POINTER(_u64), _u32)
 _sig("mvbt_last_error", ctypes.c_char_p)
 _sig("mvbt_status_string", ctypes.c_char_p, ctypes.c_int)
 
@@ -279,6 +280,15 @@ class _TreeBase:
         n = _u64(0)
         _check(lib.mvbt_copy_pool(self._h, img.ctypes.data, img.shape[0], ctypes.byref(n)), "copy_pool")
         return img[: n.value]
+
+    def stats(self) -> dict:
+        """Device counters: versions copied, splits, longest walks, epoch, error bits per site."""
+        buf = (_u64 * 23)()
+        _check(lib.mvbt_stats(self._h, buf, 23), "stats")
+        v = list(buf)
+        return {"cow": v[0], "splits": v[1], "max_hops": v[2], "max_descent": v[3], "epoch": v[4],
+                "error_bits": v[5], "error_sites": {i: v[6 + i] for i in range(16) if v[6 + i]},
+                "restarts": v[22]}
 
     def device_view(self) -> mvbt_device_view:
         v = mvbt_device_view()

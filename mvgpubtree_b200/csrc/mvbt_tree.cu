@@ -528,6 +528,19 @@ int mvbt_internal_view(mvbt_tree* t, device_tree* view, int* tile_width, int* bl
 
 void mvbt_internal_set_error(const char* msg) { g_last_error = msg ? msg : ""; }
 
+int mvbt_stats(mvbt_tree* t, uint64_t* out, uint32_t n) {
+  if (!t || !out) return fail(MVBT_ERR_BAD_ARG, "null argument");
+  MVBT_CUDA_TRY(cudaSetDevice(t->device));
+  MVBT_CUDA_TRY(cudaDeviceSynchronize());
+  control_block c;
+  MVBT_CUDA_TRY(cudaMemcpy(&c, t->ctl, sizeof(c), cudaMemcpyDeviceToHost));
+  uint64_t v[23] = {c.stat_cow, c.stat_split, c.stat_max_hops, c.stat_max_steps, c.epoch, c.error};
+  for (int i = 0; i < 16; ++i) v[6 + i] = c.err_site[i];
+  v[22] = c.stat_restarts;
+  for (uint32_t i = 0; i < n && i < 23; ++i) out[i] = v[i];
+  return MVBT_OK;
+}
+
 int mvbt_get_device_view(mvbt_tree* t, mvbt_device_view* out) {
   if (!t || !out) return fail(MVBT_ERR_BAD_ARG, "null argument");
   out->pool      = t->pool;

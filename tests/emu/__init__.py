@@ -29,6 +29,7 @@ def lib():
             "emu_range": (None, [vp, u32p, u32p, vp, vp, u32, u64, u32, i, i]),
             "emu_insert_range": (None, [vp, u32p, u32p, u64, u32p, u32p, u64, vp, vp, u32, i, i]),
             "emu_validate": (i, [vp, u32, vp]),
+            "emu_stats": (None, [vp, np.ctypeslib.ndpointer(dtype=np.uint64, flags="C_CONTIGUOUS")]),
             "emu_batch_run": (None, [vp, u32, np.ctypeslib.ndpointer(dtype=np.uint64, flags="C_CONTIGUOUS"),
                                      u32p, u32p, u32p,
                                      np.ctypeslib.ndpointer(dtype=np.uint64, flags="C_CONTIGUOUS"),
@@ -62,6 +63,12 @@ class EmuTree:
     @property
     def errors(self) -> int:
         return int(self.L.emu_errors(self.h))
+
+    def stats(self) -> dict:
+        v = np.zeros(21, np.uint64)
+        self.L.emu_stats(self.h, v)
+        return {"cow": int(v[0]), "splits": int(v[1]), "max_hops": int(v[2]), "max_descent": int(v[3]),
+                "error_sites": {i: int(v[4 + i]) for i in range(16) if v[4 + i]}, "restarts": int(v[20])}
 
     def snapshot(self) -> int:
         return int(self.L.emu_snapshot(self.h))

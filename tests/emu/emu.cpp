@@ -95,7 +95,7 @@ void* emu_create(int versioned, uint32_t capacity, uint32_t spin_limit, uint32_t
   t->pool.assign((size_t)capacity * 32, 0xA5A5A5A5u);  // garbage, as fresh cudaMalloc memory
   for (int i = 0; i < 32 * mvbt::kInitialNodes; ++i) t->pool[i] = mvbt::initial_tree_word(i);
   mvbt::init_control(t->ctl, capacity, chunk ? chunk : 8, spin_limit ? spin_limit : (1u << 20),
-                     200u * 1000u * 1000u);
+                     4000u * 1000u * 1000u);
   return t;
 }
 
@@ -103,6 +103,15 @@ void emu_destroy(void* h) { delete static_cast<emu_tree*>(h); }
 
 uint32_t emu_errors(void* h) { return static_cast<emu_tree*>(h)->ctl.error; }
 uint32_t emu_bump(void* h) { return static_cast<emu_tree*>(h)->ctl.bump; }
+void emu_stats(void* h, uint64_t* out) {
+  auto& c = static_cast<emu_tree*>(h)->ctl;
+  out[0] = c.stat_cow;
+  out[1] = c.stat_split;
+  out[2] = c.stat_max_hops;
+  out[3] = c.stat_max_steps;
+  for (int i = 0; i < 16; ++i) out[4 + i] = c.err_site[i];
+  out[20] = c.stat_restarts;
+}
 
 uint32_t emu_snapshot(void* h) {
   auto* t = static_cast<emu_tree*>(h);
