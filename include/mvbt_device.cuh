@@ -17,8 +17,11 @@
 //   take_snapshot             <- take_snapshot(tile) (include/gpu_versioned_blink_tree.hpp:332-344)
 //
 // Node format (128 bytes, 128-byte aligned, 32 words):
-//   pairs 0..13  {key, value}  leaf: key/value, interior: {separator, child index}; sorted by key,
+//   pairs 0..12  {key, value}  leaf: key/value, interior: {separator, child index}; sorted by key,
 //                              unused pairs are {0xFFFFFFFF, 0xFFFFFFFF}
+//   pair 13      {low fence, mod}     low fence = smallest key the node may hold (fixed for the
+//                                     node's life); mod = modification count, bumped and
+//                                     published before every change
 //   pair 14      {high key, link}     high key = exclusive upper fence (0xFFFFFFFF on the
 //                                     rightmost node of a level); link = bit31 lock |
 //                                     bits 0..27 right-sibling index (0x0FFFFFFF = none)
@@ -27,6 +30,12 @@
 // A tile of W threads (W = 8 or 16) holds one node in registers: lane l owns pairs
 // [l*16/W, (l+1)*16/W), so an 8-lane tile reads a node as eight 16-byte vector loads and a
 // 16-lane tile as sixteen 8-byte loads -- one 128-byte line either way.
+//
+// A node is read as several vector loads that are not one atomic access, so a node read while a
+// writer stores it can mix two versions, even inside one lane. Every visit therefore checks
+// low <= key (a mixed parent can route one child too far right; the visit then restarts from the
+// anchor) and key < high (too far left: follow the right link), and a reader that uses the data of
+// a leaf re-reads its header after a fence (see recheck_version / leaf_changed).
 //
 // Concurrency protocol (B-link, Lehman-Yao style):
 //   * readers never lock; a reader whose key is >= a node's high key follows the right link;
@@ -100,8 +109,8 @@ namespace cg = cooperative_groups;
 // Constants
 // ----------------------------------------------------------------------------------------------
 constexpr int kNodeWords      = 32;
-constexpr int kDataPairs      = 14;
-constexpr int kSplitLeft      = 8;  // a full node plus one entry (15) splits 8 | 7
+constexpr int kDataPairs      = 13;
+constexpr int kSplitLeft      = 7;  // a full node plus one entry (14) splits 7 | 7
 constexpr uint32_t kEmptyKey  = 0xFFFFFFFFu;
 constexpr uint32_t kNotFound  = 0xFFFFFFFFu;
 constexpr uint32_t kLatest    = 0xFFFFFFFFu;  // read the newest version
@@ -156,7 +165,8 @@ struct control_block {
 // a reader that sees a mix of two versions of any node still finds a valid route.
 MVBT_HD uint32_t initial_tree_word(int t) {
   const int node = t >> 5, w = t & 31;
-  if (w < 28) {
+  if (w == 26 || w == 27) return 0u;                 // low fence 0, modification count 0
+  if (w < 26) {
     if (w == 0) return 0u;                           // first key: 0
     if (w == 1) return node == 0 ? kFirstLeaf : 0u;  // anchor -> leaf 1; tombstone value 0
     return kEmptyKey;
@@ -297,6 +307,8 @@ MVBT_DEV void st_lane(uint32_t* p, const node_regs<W>& n) {
 template <int W>
 struct layout {
   static constexpr int P          = 16 / W;
+  static constexpr int kFenceLane = 13 / P;  // lane owning pair 13 {low, mod}
+  static constexpr int kFenceSlot = 13 % P;
   static constexpr int kLinkLane  = 14 / P;  // lane owning pair 14 {high, link}
   static constexpr int kLinkSlot  = 14 % P;
   static constexpr int kVerLane   = 15 / P;  // lane owning pair 15 {ts, older|level}
@@ -307,17 +319,33 @@ struct header {
   uint32_t high;
   uint32_t link;
   uint32_t ts;
-  uint32_t ol;  // older | level << 28
+  uint32_t ol;   // older | level << 28
+  uint32_t low;  // low fence: every key of the node is >= low (fixed for the life of the node)
+  uint32_t mod;  // modification count, published before every change of the node
   MVBT_DEV uint32_t level() const { return ol >> 28; }
   MVBT_DEV uint32_t older() const { return ol & kIndexMask; }
   MVBT_DEV uint32_t sibling() const { return link & kIndexMask; }
   MVBT_DEV bool is_leaf() const { return level() == 0; }
 };
 
+MVBT_DEV header make_header(uint32_t low, uint32_t mod, uint32_t high, uint32_t link, uint32_t ts,
+                            uint32_t ol) {
+  header h;
+  h.low  = low;
+  h.mod  = mod;
+  h.high = high;
+  h.link = link;
+  h.ts   = ts;
+  h.ol   = ol;
+  return h;
+}
+
 template <int W, class Tile>
 MVBT_DEV header get_header(const node_regs<W>& n, const Tile& t) {
   using L = layout<W>;
   header h;
+  h.low  = t.shfl(n.k[L::kFenceSlot], L::kFenceLane);
+  h.mod  = t.shfl(n.v[L::kFenceSlot], L::kFenceLane);
   h.high = t.shfl(n.k[L::kLinkSlot], L::kLinkLane);
   h.link = t.shfl(n.v[L::kLinkSlot], L::kLinkLane);
   h.ts   = t.shfl(n.k[L::kVerSlot], L::kVerLane);
@@ -329,6 +357,10 @@ template <int W, class Tile>
 MVBT_DEV void set_header(node_regs<W>& n, const header& h, const Tile& t) {
   using L      = layout<W>;
   const int r  = t.thread_rank();
+  if (r == L::kFenceLane) {
+    n.k[L::kFenceSlot] = h.low;
+    n.v[L::kFenceSlot] = h.mod;
+  }
   if (r == L::kLinkLane) {
     n.k[L::kLinkSlot] = h.high;
     n.v[L::kLinkSlot] = h.link;
@@ -530,7 +562,8 @@ struct device_tree {
   MVBT_DEV void store_header(uint32_t idx, const node_regs<W>& n, const Tile& t) const {
     using L     = layout<W>;
     const int r = t.thread_rank();
-    if (r == L::kLinkLane || r == L::kVerLane) st_lane<W>(node_ptr(idx) + r * (32 / W), n);
+    if (r == L::kFenceLane || r == L::kLinkLane || r == L::kVerLane)
+      st_lane<W>(node_ptr(idx) + r * (32 / W), n);
   }
 
   // Records error bits and counts the site that raised them (control_block::err_site).
@@ -625,32 +658,29 @@ struct device_tree {
   // ---- versioning ----
   // Makes the version visible to older snapshots immutable before node idx (locked, content n)
   // is changed in epoch E: copies n to a fresh node and publishes {ts = E, older = copy}.
-  // On a plain tree the ts word counts modifications instead: it is bumped and published before
-  // the data changes, so a concurrent reader that re-reads it after a fence sees any change.
+  // Every change of a node first bumps and publishes its modification count (and, on a versioned
+  // tree, the first change in epoch E copies the node to a fresh node O and publishes
+  // {ts = E, older = O} with it), then fences, so a concurrent reader that re-reads the header
+  // after reading the data sees that something changed.
   template <int W, class Tile>
   MVBT_DEV bool prepare_write(uint32_t idx, node_regs<W>& n, header& h, uint32_t E, const Tile& t) const {
-    if (!versioned) {
-      h.ts += 1;
-      set_header<W>(n, h, t);
-      store_header<W>(idx, n, t);
+    if (versioned && h.ts != E) {
+      uint32_t copy = alloc(t);
+      if (copy == kNone) return false;
+      node_regs<W> c = n;
+      header hc      = h;
+      hc.link &= ~kLockBit;
+      set_header<W>(c, hc, t);
+      store<W>(copy, c, t);
       __threadfence();
-      return true;
+      h.ts = E;
+      h.ol = (h.ol & ~kIndexMask) | copy;
+      if (t.thread_rank() == 0) atomicAdd(&ctl->stat_cow, 1ull);
     }
-    if (h.ts == E) return true;
-    uint32_t copy = alloc(t);
-    if (copy == kNone) return false;
-    node_regs<W> c = n;
-    header hc      = h;
-    hc.link &= ~kLockBit;
-    set_header<W>(c, hc, t);
-    store<W>(copy, c, t);
-    __threadfence();
-    h.ts = E;
-    h.ol = (h.ol & ~kIndexMask) | copy;
+    h.mod += 1;
     set_header<W>(n, h, t);
     store_header<W>(idx, n, t);
     __threadfence();
-    if (t.thread_rank() == 0) atomicAdd(&ctl->stat_cow, 1ull);
     return true;
   }
 
@@ -679,13 +709,14 @@ struct device_tree {
   // ts <= snapshot re-reads the header after a fence. A writer publishes {ts = E, older = copy}
   // before it changes the data, so if any lane saw changed data the re-read shows ts > snapshot:
   // the reader then returns the index of the immutable copy (else kNone: the data is consistent).
-  // The plain-tree counterpart: true if the modification count of leaf idx is no longer `seen`.
+  // For readers of the newest state: true if the modification count of leaf idx is no longer
+  // `seen` (a writer changed it while it was being read).
   template <class Tile>
   MVBT_DEV bool leaf_changed(uint32_t idx, uint32_t seen, const Tile& t) const {
     __threadfence();
     t.sync();
     uint32_t now = 0;
-    if (t.thread_rank() == 0) now = ld_relaxed_u32(node_ptr(idx) + 30);
+    if (t.thread_rank() == 0) now = ld_relaxed_u32(node_ptr(idx) + 27);
     return t.shfl(now, 0) != seen;
   }
 
@@ -718,6 +749,10 @@ struct device_tree {
       bool copy = via_older;
       via_older = false;
       if (snap && !to_version<W>(idx, n, h, ts, concurrent, copy, t)) return kNotFound;
+      if (key < h.low) {  // routed too far right by a torn read upstream: start over
+        idx = kAnchor;
+        continue;
+      }
       if (key >= h.high && h.sibling() != kNone) {
         idx = h.sibling();
         continue;
@@ -730,12 +765,13 @@ struct device_tree {
             via_older = true;
             continue;
           }
-        } else if (!versioned && concurrent && leaf_changed(idx, h.ts, t)) {
+        } else if (!snap && concurrent && leaf_changed(idx, h.mod, t)) {
           continue;  // a writer changed the leaf while it was read: read it again
         }
         return leaf_value<W>(n, key, t);
       }
       idx = child_for<W>(n, key, t);
+      if (idx == kNone) idx = kAnchor;
     }
     if (t.thread_rank() == 0) set_error(kErrStepLimit, 4);
     return kNotFound;
@@ -767,6 +803,10 @@ struct device_tree {
       bool copy = via_older;
       via_older = false;
       if (snap && !to_version<W>(idx, n, h, ts, concurrent, copy, t)) return 0;
+      if (lo < h.low) {
+        idx = kAnchor;
+        continue;
+      }
       if (lo >= h.high && h.sibling() != kNone) {
         idx = h.sibling();
         continue;
@@ -779,12 +819,13 @@ struct device_tree {
             via_older = true;
             continue;
           }
-        } else if (!versioned && concurrent && leaf_changed(idx, h.ts, t)) {
+        } else if (!snap && concurrent && leaf_changed(idx, h.mod, t)) {
           continue;
         }
         break;
       }
       idx = child_for<W>(n, lo, t);
+      if (idx == kNone) idx = kAnchor;
     }
     // scan leaves to the right (a sibling chain is never longer than the pool)
     uint32_t count = 0;
@@ -834,7 +875,7 @@ struct device_tree {
             via_older = true;
             continue;
           }
-        } else if (!versioned && concurrent && leaf_changed(idx, h.ts, t)) {
+        } else if (!snap && concurrent && leaf_changed(idx, h.mod, t)) {
           continue;
         }
         settled = true;
@@ -867,6 +908,13 @@ struct device_tree {
         top_level = h.level();
         first     = false;
       }
+      if (key < h.low) {  // routed too far right by a torn read: start over from the anchor
+        idx   = kAnchor;
+        first = true;
+        path0 = kNone;
+        path1 = kNone;
+        continue;
+      }
       if (key >= h.high && h.sibling() != kNone) {
         idx = h.sibling();
         continue;
@@ -882,6 +930,7 @@ struct device_tree {
         if (t.thread_rank() == (int)(lvl - W)) path1 = idx;
       }
       idx = child_for<W>(n, key, t);
+      if (idx == kNone) idx = kAnchor;
     }
     if (t.thread_rank() == 0) set_error(kErrStepLimit, 8);
     return kNone;
@@ -900,6 +949,11 @@ struct device_tree {
       if (!valid(idx, t)) return kNone;
       load<W>(idx, n, true, t);
       h = get_header<W>(n, t);
+      if (key < h.low) {
+        idx   = kAnchor;
+        chase = 0;
+        continue;
+      }
       if (key >= h.high && h.sibling() != kNone) {
         if (++chase > kChaseRestart) {
           idx   = kAnchor;
@@ -916,6 +970,7 @@ struct device_tree {
       }
       idx   = child_for<W>(n, key, t);
       chase = 0;
+      if (idx == kNone) idx = kAnchor;
     }
     if (t.thread_rank() == 0) set_error(kErrStepLimit, 12);
     return kNone;
@@ -934,8 +989,9 @@ struct device_tree {
       if (!lock(idx, t)) return kNone;
       load<W>(idx, n, true, t);
       h = get_header<W>(n, t);
-      if (h.level() != level) {  // only the anchor changes level: re-approach from it
+      if (h.level() != level || key < h.low) {  // the anchor grew, or the approach was misrouted
         unlock(idx, t);
+        if (key < h.low) idx = kAnchor;
         continue;
       }
       uint32_t hops = 0;
@@ -984,8 +1040,9 @@ struct device_tree {
     build_from_merged<W>(n, pos, key, val, 0, kSplitLeft, left, t);
     build_from_merged<W>(n, pos, key, val, kSplitLeft, kDataPairs + 1 - kSplitLeft, right, t);
     uint32_t rmin = t.shfl(right.k[0], 0);
-    header hr{h.high, h.sibling(), ts, (h.level() << 28) | (versioned ? h.older() : kNone)};
-    header hl{rmin, r | kLockBit, h.ts, h.ol};
+    header hr = make_header(rmin, 0u, h.high, h.sibling(), ts,
+                            (h.level() << 28) | (versioned ? h.older() : kNone));
+    header hl = make_header(h.low, h.mod, rmin, r | kLockBit, h.ts, h.ol);
     set_header<W>(right, hr, t);
     set_header<W>(left, hl, t);
     store<W>(r, right, t);
@@ -1018,7 +1075,7 @@ struct device_tree {
       x.k[j]      = q == 0 ? 0u : (q == 1 ? sep_key : kEmptyKey);
       x.v[j]      = q == 0 ? old_top : (q == 1 ? sep_child : kEmptyKey);
     }
-    header hx{kEmptyKey, kNone, versioned ? E : 0u, (lvl << 28) | older};
+    header hx = make_header(0u, 0u, kEmptyKey, kNone, versioned ? E : 0u, (lvl << 28) | older);
     set_header<W>(x, hx, t);
     store<W>(top, x, t);
     __threadfence();

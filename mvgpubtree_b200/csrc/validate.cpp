@@ -4,7 +4,8 @@
 // at the requested snapshot and checks, level by level from the root: key order inside nodes,
 // that every key lies in [low fence, high key), levels, right links (the last node of a level has
 // high key 0xFFFFFFFF and no sibling), that no node is left locked, and that every node of a level
-// is referenced by exactly one entry of the level above. Unlike the reference it needs no
+// is referenced by exactly one entry of the level above, and that each node's stored low fence
+// equals the high key of its left neighbour. Unlike the reference it needs no
 // allocator bookkeeping, so it works for every pool layout.
 #include <algorithm>
 #include <iterator>
@@ -22,12 +23,13 @@ constexpr uint32_t kEmpty = 0xFFFFFFFFu;
 constexpr uint32_t kNone  = 0x0FFFFFFFu;
 constexpr uint32_t kMask  = 0x0FFFFFFFu;
 constexpr uint32_t kLock  = 0x80000000u;
-constexpr int kData       = 14;
+constexpr int kData       = 13;
 
 struct host_node {
   const uint32_t* w;
   uint32_t key(int p) const { return w[2 * p]; }
   uint32_t val(int p) const { return w[2 * p + 1]; }
+  uint32_t low() const { return w[26]; }
   uint32_t high() const { return w[28]; }
   uint32_t link() const { return w[29]; }
   uint32_t ts() const { return w[30]; }
@@ -92,6 +94,10 @@ extern "C" int mvbt_validate_image_detail(const uint32_t* img, uint64_t nn, int 
       if ((int)x.level() != level) {
         ++violations;
         note("level", level, slot, x.level(), 0);
+      }
+      if (x.low() != low) {
+        ++violations;
+        note("stored-low-fence", level, slot, x.low(), low);
       }
       if (x.link() & kLock) ++rep->locked_nodes;
       uint32_t prev = 0;
