@@ -82,6 +82,12 @@ template <class T, class U>
 inline T atomicAdd(T* p, U v) { return __atomic_fetch_add(p, (T)v, __ATOMIC_SEQ_CST); }
 template <class T, class U>
 inline T atomicExch(T* p, U v) { return __atomic_exchange_n(p, (T)v, __ATOMIC_SEQ_CST); }
+template <class T, class U, class V>
+inline T atomicCAS(T* p, U expected, V desired) {
+  T e = (T)expected;
+  __atomic_compare_exchange_n(p, &e, (T)desired, false, __ATOMIC_SEQ_CST, __ATOMIC_SEQ_CST);
+  return e;
+}
 template <class T, class U>
 inline T atomicMax(T* p, U v) {
   T cur = __atomic_load_n(p, __ATOMIC_RELAXED);
@@ -1253,81 +1259,157 @@ MVBT_DEV bool run_batch_op(const device_tree& T, const batch_view& B, uint64_t i
   return write;
 }
 
-// Schedule of the persistent batched launch: claim positions run batch by batch, writes first
-// inside each batch (perm maps a claim position to an op index), and a batch may start only
-// once every write of the previous batch has finished.
+// Schedule of the persistent batched launch. Within each batch the claim order puts writes first
+// (perm maps a claim position to an op index). Writes of batch b may start once every write of
+// the batches before b has finished, reads of batch b likewise (they read the state after those
+// writes; writes of b and later batches go into newer versions, so the reads may lag behind).
+// Two device queues hand out work: write ordinals (the critical path, small claims, served first)
+// and read ordinals (larger claims, taken when no write is ready). done_batches counts the leading
+// batches whose writes are all finished.
 struct batch_sched {
-  const uint64_t* batch_off;  // [num_batches + 1] claim positions of each batch
-  const uint32_t* perm;       // claim position -> op index
-  const uint32_t* n_writes;   // [num_batches] writes per batch
-  uint32_t* writes_done;      // [num_batches] finished writes (zero at launch)
-  unsigned long long* cursor; // next unclaimed position (zero at launch)
-  const uint32_t* params;     // device words: [0] num_batches, [1] snapshot of batch 0
-  uint32_t chunk;             // positions claimed per tile at a time
+  const uint64_t* batch_off;     // [nb + 1] claim positions of each batch
+  const uint32_t* perm;          // claim position -> op index
+  const uint32_t* n_writes;      // [nb] writes per batch
+  const uint64_t* wpre;          // [nb + 1] first write ordinal of each batch
+  const uint64_t* rpre;          // [nb + 1] first read ordinal of each batch
+  uint32_t* writes_done;         // [nb] finished writes (zero at launch)
+  uint32_t* done_batches;        // zero at launch
+  unsigned long long* wcursor;   // next write ordinal (zero at launch)
+  unsigned long long* rcursor;   // next read ordinal (zero at launch)
+  const uint32_t* params;        // [0] num_batches, [1] snapshot of batch 0
 };
+
+constexpr uint32_t kWriteClaim = 2;
+constexpr uint32_t kReadClaim  = 8;
+
+// Largest b in [lo, nb) with pre[b] <= x (pre is non-decreasing), starting from the hint lo.
+MVBT_DEV uint32_t batch_of_ordinal(const uint64_t* pre, uint32_t nb, uint64_t x, uint32_t lo) {
+  if (lo >= nb) lo = 0;
+  if (pre[lo] > x) lo = 0;
+  if (lo + 1 < nb && pre[lo + 1] > x) return lo;
+  uint32_t hi = nb;
+  while (hi - lo > 1) {
+    uint32_t mid = (lo + hi) >> 1;
+    if (pre[mid] <= x) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// Advances done_batches past every leading batch whose writes are all finished (lane 0 only).
+MVBT_DEV void advance_done(const batch_sched& sc, uint32_t nb) {
+  uint32_t d = ld_relaxed_u32(sc.done_batches);
+  while (d < nb) {
+    if (ld_relaxed_u32(&sc.writes_done[d]) < sc.n_writes[d]) break;
+    __threadfence();
+    uint32_t prev = atomicCAS(sc.done_batches, d, d + 1);
+    d = (prev == d) ? d + 1 : prev;
+  }
+}
+
+// Waits (bounded) until the writes of every batch before b have finished; returns false on timeout.
+template <class Tile>
+MVBT_DEV bool wait_batch_ready(const device_tree& T, const batch_sched& sc, uint32_t nb, uint32_t b,
+                               const Tile& t) {
+  const unsigned long long t0 = global_ns();
+  for (uint32_t w = 0;; ++w) {
+    uint32_t d = 0;
+    if (t.thread_rank() == 0) {
+      advance_done(sc, nb);
+      d = ld_relaxed_u32(sc.done_batches);
+    }
+    d = t.shfl(d, 0);
+    if (d >= b) {
+      __threadfence();
+      return true;
+    }
+    if (global_ns() - t0 > T.ctl->wait_ns) return false;
+    __nanosleep(w < 8 ? 128 : 1024);
+  }
+}
 
 // Worker loop of one tile in the persistent batched launch.
 template <int W, class Tile>
 MVBT_DEV void batched_worker(const device_tree& T, const batch_view& B, const batch_sched& sc,
                              const Tile& t) {
-  const uint32_t nb    = ld_relaxed_u32(sc.params + 0);
-  const uint32_t S0    = ld_relaxed_u32(sc.params + 1);
-  const uint64_t total = sc.batch_off[nb];
-  uint32_t b           = 0;   // batch of the current position (positions only grow)
-  uint32_t ready       = 0;   // every batch < ready may run
-  uint32_t pending     = 0;   // finished writes of batch b not yet published
-  const unsigned long long lns = T.ctl->wait_ns;
-  for (;;) {
-    unsigned long long base = 0;
-    if (t.thread_rank() == 0) base = atomicAdd(sc.cursor, (unsigned long long)sc.chunk);
-    base = t.shfl(base, 0);
-    if (base >= total) break;
-    const uint64_t end = base + sc.chunk < total ? base + sc.chunk : total;
-    for (uint64_t p = base; p < end; ++p) {
-      while (p >= sc.batch_off[b + 1]) {
-        if (pending && t.thread_rank() == 0) atomicAdd(&sc.writes_done[b], pending);
-        pending = 0;
-        ++b;
-      }
-      if (b >= ready) {
-        // publish own finished writes first, then wait for the previous batch's writes
-        if (pending) {
-          __threadfence();
-          if (t.thread_rank() == 0) atomicAdd(&sc.writes_done[b], pending);
-          pending = 0;
-        }
-        if (b > 0) {
-          const unsigned long long t0 = global_ns();
-          bool ok = false;
-          for (uint32_t w = 0;; ++w) {
-            uint32_t done = 0;
-            if (t.thread_rank() == 0) done = ld_relaxed_u32(&sc.writes_done[b - 1]);
-            done = t.shfl(done, 0);
-            if (done >= sc.n_writes[b - 1]) {
-              ok = true;
-              break;
+  const uint32_t nb = ld_relaxed_u32(sc.params + 0);
+  const uint32_t S0 = ld_relaxed_u32(sc.params + 1);
+  const uint64_t TW = sc.wpre[nb], TR = sc.rpre[nb];
+  uint32_t wb = 0, rb = 0;  // batch hints for the two queues
+  unsigned long long idle_since = 0;
+  for (uint32_t spin = 0;;) {
+    uint32_t d = 0;
+    unsigned long long g = 0, r = 0;
+    if (t.thread_rank() == 0) {
+      d = ld_relaxed_u32(sc.done_batches);
+      g = ld_relaxed_u64(sc.wcursor);
+      r = ld_relaxed_u64(sc.rcursor);
+    }
+    d = t.shfl(d, 0);
+    g = t.shfl(g, 0);
+    r = t.shfl(r, 0);
+    if (g >= TW && r >= TR) break;
+    bool did = false;
+    // writes first: they gate every later batch
+    if (g < TW) {
+      wb = batch_of_ordinal(sc.wpre, nb, g, wb);
+      if (wb <= d) {
+        unsigned long long g0 = 0;
+        if (t.thread_rank() == 0) g0 = atomicAdd(sc.wcursor, (unsigned long long)kWriteClaim);
+        g0 = t.shfl(g0, 0);
+        for (unsigned long long x = g0; x < g0 + kWriteClaim && x < TW; ++x) {
+          wb = batch_of_ordinal(sc.wpre, nb, x, wb);
+          if (wb > d) {
+            if (!wait_batch_ready(T, sc, nb, wb, t)) {
+              if (t.thread_rank() == 0) T.set_error(kErrSpinLimit, 14);
             }
-            if (global_ns() - t0 > lns) break;
-            __nanosleep(w < 16 ? 64 : 256);
+            d = wb;
           }
-          if (!ok) {
-            if (t.thread_rank() == 0) T.set_error(kErrSpinLimit, 14);
-          }
+          const uint32_t i = sc.perm[sc.batch_off[wb] + (x - sc.wpre[wb])];
+          run_batch_op<W>(T, B, i, S0 + wb, S0 + wb + 1, t);
           __threadfence();
+          if (t.thread_rank() == 0) {
+            uint32_t c = atomicAdd(&sc.writes_done[wb], 1u) + 1u;
+            if (c == sc.n_writes[wb]) advance_done(sc, nb);
+          }
         }
-        ready = b + 1;
-      }
-      const uint32_t i = sc.perm[p];
-      if (run_batch_op<W>(T, B, i, S0 + b, S0 + b + 1, t)) {
-        __threadfence();
-        ++pending;
+        did = g0 < TW;
       }
     }
-    if (pending) {
-      __threadfence();
-      if (t.thread_rank() == 0) atomicAdd(&sc.writes_done[b], pending);
-      pending = 0;
+    if (!did && r < TR) {
+      rb = batch_of_ordinal(sc.rpre, nb, r, rb);
+      if (rb <= d) {
+        unsigned long long r0 = 0;
+        if (t.thread_rank() == 0) r0 = atomicAdd(sc.rcursor, (unsigned long long)kReadClaim);
+        r0 = t.shfl(r0, 0);
+        for (unsigned long long x = r0; x < r0 + kReadClaim && x < TR; ++x) {
+          rb = batch_of_ordinal(sc.rpre, nb, x, rb);
+          if (rb > d) {
+            if (!wait_batch_ready(T, sc, nb, rb, t)) {
+              if (t.thread_rank() == 0) T.set_error(kErrSpinLimit, 14);
+            }
+            d = rb;
+          }
+          const uint32_t i = sc.perm[sc.batch_off[rb] + sc.n_writes[rb] + (x - sc.rpre[rb])];
+          run_batch_op<W>(T, B, i, S0 + rb, S0 + rb + 1, t);
+        }
+        did = r0 < TR;
+      }
     }
+    if (did) {
+      spin       = 0;
+      idle_since = 0;
+      continue;
+    }
+    // nothing runnable yet: help advance done_batches, then back off (bounded)
+    if (t.thread_rank() == 0) advance_done(sc, nb);
+    if (idle_since == 0) idle_since = global_ns();
+    if (global_ns() - idle_since > T.ctl->wait_ns) {
+      if (t.thread_rank() == 0) T.set_error(kErrSpinLimit, 14);
+      break;
+    }
+    __nanosleep(spin < 8 ? 256 : 2048);
+    ++spin;
   }
 }
 

@@ -32,8 +32,10 @@ struct mvbt_batch_plan {
   uint64_t* d_batch_off;  // [max_batches + 1]
   uint32_t* d_params;     // [0] num_batches, [1] snapshot of batch 0
   uint32_t* d_perm;       // [max_ops]
-  uint32_t* d_counts;     // n_writes | writes_done | write fill | read fill, each [max_batches]
-  unsigned long long* d_cursor;
+  uint32_t* d_counts;     // n_writes | writes_done | write fill | read fill (each [max_batches]),
+                          // then done_batches
+  uint64_t* d_pre;        // write-ordinal prefix [max_batches + 1] | read-ordinal prefix [...]
+  unsigned long long* d_cursor;  // write cursor, read cursor
   // pinned staging
   uint64_t* h_batch_off;
   uint32_t* h_params;
@@ -122,6 +124,45 @@ __global__ void k_place(const uint32_t* __restrict__ type, const uint64_t* __res
   }
 }
 
+// First write / read ordinal of every batch (one block; exclusive scans over the batches).
+__global__ void __launch_bounds__(1024) k_prefix(const uint64_t* __restrict__ off,
+                                                 const uint32_t* __restrict__ params,
+                                                 const uint32_t* __restrict__ n_writes, uint64_t* wpre,
+                                                 uint64_t* rpre) {
+  __shared__ uint64_t sw[1024], sr[1024];
+  const uint32_t nb   = params[0];
+  const uint32_t per  = (nb + blockDim.x - 1) / blockDim.x;
+  const uint32_t b0   = threadIdx.x * per;
+  const uint32_t b1   = b0 + per < nb ? b0 + per : nb;
+  uint64_t w = 0, r = 0;
+  for (uint32_t b = b0; b < b1; ++b) {
+    w += n_writes[b];
+    r += (off[b + 1] - off[b]) - n_writes[b];
+  }
+  sw[threadIdx.x] = w;
+  sr[threadIdx.x] = r;
+  __syncthreads();
+  for (uint32_t d = 1; d < blockDim.x; d <<= 1) {
+    uint64_t aw = threadIdx.x >= d ? sw[threadIdx.x - d] : 0;
+    uint64_t ar = threadIdx.x >= d ? sr[threadIdx.x - d] : 0;
+    __syncthreads();
+    sw[threadIdx.x] += aw;
+    sr[threadIdx.x] += ar;
+    __syncthreads();
+  }
+  uint64_t pw = threadIdx.x ? sw[threadIdx.x - 1] : 0, pr = threadIdx.x ? sr[threadIdx.x - 1] : 0;
+  for (uint32_t b = b0; b < b1; ++b) {
+    wpre[b] = pw;
+    rpre[b] = pr;
+    pw += n_writes[b];
+    pr += (off[b + 1] - off[b]) - n_writes[b];
+  }
+  if (threadIdx.x == blockDim.x - 1) {
+    wpre[nb] = sw[blockDim.x - 1];
+    rpre[nb] = sr[blockDim.x - 1];
+  }
+}
+
 __global__ void k_batch_begin(mvbt::control_block* ctl, uint32_t* params) {
   if (threadIdx.x == 0) {
     __threadfence();
@@ -183,24 +224,31 @@ int enqueue_persistent(mvbt_batch_plan* p, const launch_ctx& c, const batch_view
   MVBT_TRY(cudaMemcpyAsync(p->d_batch_off, p->h_batch_off, (mb + 1) * sizeof(uint64_t),
                            cudaMemcpyHostToDevice, s));
   MVBT_TRY(cudaMemcpyAsync(p->d_params, p->h_params, 2 * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
-  MVBT_TRY(cudaMemsetAsync(p->d_counts, 0, 4ull * mb * sizeof(uint32_t), s));
-  MVBT_TRY(cudaMemsetAsync(p->d_cursor, 0, sizeof(unsigned long long), s));
+  MVBT_TRY(cudaMemsetAsync(p->d_counts, 0, (4ull * mb + 4) * sizeof(uint32_t), s));
+  MVBT_TRY(cudaMemsetAsync(p->d_cursor, 0, 2 * sizeof(unsigned long long), s));
   uint32_t* nw    = p->d_counts;
   uint32_t* wdone = p->d_counts + mb;
   uint32_t* wfill = p->d_counts + 2 * mb;
   uint32_t* rfill = p->d_counts + 3 * mb;
+  uint32_t* done  = p->d_counts + 4 * mb;
+  uint64_t* wpre  = p->d_pre;
+  uint64_t* rpre  = p->d_pre + (mb + 1);
   k_count_writes<<<kPrepassBlocks, kPrepassThreads, 0, s>>>(B.type, p->d_batch_off, p->d_params, nw);
   k_place<<<kPrepassBlocks, kPrepassThreads, 0, s>>>(B.type, p->d_batch_off, p->d_params, nw, wfill,
                                                      rfill, p->d_perm);
+  k_prefix<<<1, 1024, 0, s>>>(p->d_batch_off, p->d_params, nw, wpre, rpre);
   k_batch_begin<<<1, 32, 0, s>>>(c.ctl, p->d_params);
   batch_sched sc;
-  sc.batch_off   = p->d_batch_off;
-  sc.perm        = p->d_perm;
-  sc.n_writes    = nw;
-  sc.writes_done = wdone;
-  sc.cursor      = p->d_cursor;
-  sc.params      = p->d_params;
-  sc.chunk       = 16;
+  sc.batch_off    = p->d_batch_off;
+  sc.perm         = p->d_perm;
+  sc.n_writes     = nw;
+  sc.wpre         = wpre;
+  sc.rpre         = rpre;
+  sc.writes_done  = wdone;
+  sc.done_batches = done;
+  sc.wcursor      = p->d_cursor;
+  sc.rcursor      = p->d_cursor + 1;
+  sc.params       = p->d_params;
   const int slot = (int)(p->timed_runs % mvbt_batch_plan::kTimed);
   if (p->timing) cudaEventRecord(p->ev_begin[slot], s);
   if (c.W == 8) {
@@ -240,8 +288,9 @@ int mvbt_batch_plan_create(mvbt_tree* tree, uint64_t max_ops, uint32_t max_batch
   bool ok = cudaMalloc(&p->d_batch_off, (max_batches + 1) * sizeof(uint64_t)) == cudaSuccess &&
             cudaMalloc(&p->d_params, 64) == cudaSuccess &&
             cudaMalloc(&p->d_perm, max_ops * sizeof(uint32_t)) == cudaSuccess &&
-            cudaMalloc(&p->d_counts, 4ull * max_batches * sizeof(uint32_t)) == cudaSuccess &&
-            cudaMalloc(&p->d_cursor, sizeof(unsigned long long)) == cudaSuccess &&
+            cudaMalloc(&p->d_counts, (4ull * max_batches + 4) * sizeof(uint32_t)) == cudaSuccess &&
+            cudaMalloc(&p->d_pre, 2ull * (max_batches + 1) * sizeof(uint64_t)) == cudaSuccess &&
+            cudaMalloc(&p->d_cursor, 2 * sizeof(unsigned long long)) == cudaSuccess &&
             cudaMallocHost(&p->h_batch_off, (max_batches + 1) * sizeof(uint64_t)) == cudaSuccess &&
             cudaMallocHost(&p->h_params, 64) == cudaSuccess;
   if (!ok) {
@@ -261,6 +310,7 @@ int mvbt_batch_plan_destroy(mvbt_batch_plan* p) {
   cudaFree(p->d_params);
   cudaFree(p->d_perm);
   cudaFree(p->d_counts);
+  cudaFree(p->d_pre);
   cudaFree(p->d_cursor);
   cudaFreeHost(p->h_batch_off);
   cudaFreeHost(p->h_params);

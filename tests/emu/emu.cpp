@@ -208,16 +208,21 @@ void emu_batch_run(void* h, uint32_t nb, const uint64_t* off, const uint32_t* ty
     return;
   }
   std::vector<uint32_t> perm(off[nb]), n_writes(nb, 0), writes_done(nb, 0);
+  std::vector<uint64_t> wpre(nb + 1, 0), rpre(nb + 1, 0);
   for (uint32_t b = 0; b < nb; ++b) {
     uint64_t pos = off[b];
     for (uint64_t i = off[b]; i < off[b + 1]; ++i)
       if (mvbt::is_write_op(type[i])) perm[pos++] = (uint32_t)i, ++n_writes[b];
     for (uint64_t i = off[b]; i < off[b + 1]; ++i)
       if (!mvbt::is_write_op(type[i])) perm[pos++] = (uint32_t)i;
+    wpre[b + 1] = wpre[b] + n_writes[b];
+    rpre[b + 1] = rpre[b] + (off[b + 1] - off[b]) - n_writes[b];
   }
-  unsigned long long cursor = 0;
-  uint32_t params[2]        = {nb, t->ctl.epoch};
-  mvbt::batch_sched sc{off, perm.data(), n_writes.data(), writes_done.data(), &cursor, params, 4};
+  unsigned long long cursors[2] = {0, 0};
+  uint32_t done                 = 0;
+  uint32_t params[2]            = {nb, t->ctl.epoch};
+  mvbt::batch_sched sc{off, perm.data(), n_writes.data(), wpre.data(), rpre.data(), writes_done.data(),
+                       &done, &cursors[0], &cursors[1], params};
   EMU_DISPATCH(W, run((uint64_t)tiles, tiles, kW, [&](uint64_t, const emu_tile& tile) {
     mvbt::batched_worker<kW>(v, B, sc, tile);
   }));
