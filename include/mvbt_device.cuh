@@ -573,6 +573,16 @@ struct device_tree {
   }
 
   // Records error bits and counts the site that raised them (control_block::err_site).
+  // Orders every lane's earlier stores before any lane's later ones. A fence orders only the
+  // calling thread's own accesses; the warp barrier after it carries that order across the lanes
+  // of the tile, so a store that publishes a node (a link, a header) is never visible before the
+  // stores of other lanes that wrote what it points to.
+  template <class Tile>
+  MVBT_DEV void publish_fence(const Tile& t) const {
+    __threadfence();
+    t.sync();
+  }
+
   MVBT_DEV void set_error(uint32_t bits, uint32_t site = 0) const {
     atomicOr(&ctl->error, bits);
     atomicAdd(&ctl->err_site[site & 15], 1u);
@@ -678,7 +688,7 @@ struct device_tree {
       hc.link &= ~kLockBit;
       set_header<W>(c, hc, t);
       store<W>(copy, c, t);
-      __threadfence();
+      publish_fence(t);
       h.ts = E;
       h.ol = (h.ol & ~kIndexMask) | copy;
       if (t.thread_rank() == 0) atomicAdd(&ctl->stat_cow, 1ull);
@@ -686,7 +696,7 @@ struct device_tree {
     h.mod += 1;
     set_header<W>(n, h, t);
     store_header<W>(idx, n, t);
-    __threadfence();
+    publish_fence(t);
     return true;
   }
 
@@ -1052,7 +1062,7 @@ struct device_tree {
     set_header<W>(right, hr, t);
     set_header<W>(left, hl, t);
     store<W>(r, right, t);
-    __threadfence();
+    publish_fence(t);
     store<W>(idx, left, t);
     if (t.thread_rank() == 0) atomicAdd(&ctl->stat_split, 1ull);
     unlock(idx, t);
@@ -1084,7 +1094,7 @@ struct device_tree {
     header hx = make_header(0u, 0u, kEmptyKey, kNone, versioned ? E : 0u, (lvl << 28) | older);
     set_header<W>(x, hx, t);
     store<W>(top, x, t);
-    __threadfence();
+    publish_fence(t);
 #pragma unroll
     for (int j = 0; j < 16 / W; ++j)
       if (pair_index<W>(t, j) == 0) n.v[j] = top;
@@ -1321,6 +1331,7 @@ MVBT_DEV bool wait_batch_ready(const device_tree& T, const batch_sched& sc, uint
     d = t.shfl(d, 0);
     if (d >= b) {
       __threadfence();
+      t.sync();
       return true;
     }
     if (global_ns() - t0 > T.ctl->wait_ns) return false;
@@ -1349,6 +1360,8 @@ MVBT_DEV void batched_worker(const device_tree& T, const batch_view& B, const ba
     g = t.shfl(g, 0);
     r = t.shfl(r, 0);
     if (g >= TW && r >= TR) break;
+    __threadfence();  // the batches counted in d are finished: see their writes
+    t.sync();
     bool did = false;
     // writes first: they gate every later batch
     if (g < TW) {
@@ -1368,6 +1381,7 @@ MVBT_DEV void batched_worker(const device_tree& T, const batch_view& B, const ba
           const uint32_t i = sc.perm[sc.batch_off[wb] + (x - sc.wpre[wb])];
           run_batch_op<W>(T, B, i, S0 + wb, S0 + wb + 1, t);
           __threadfence();
+          t.sync();
           if (t.thread_rank() == 0) {
             uint32_t c = atomicAdd(&sc.writes_done[wb], 1u) + 1u;
             if (c == sc.n_writes[wb]) advance_done(sc, nb);
