@@ -53,6 +53,8 @@ def parse_args():
     ap.add_argument("--batches", type=int, default=256)
     ap.add_argument("--seed", type=int, default=20240611)
     ap.add_argument("--tile-width", type=int, default=8)
+    ap.add_argument("--blocks-per-sm", type=int, default=0,
+                    help="0 = full occupancy of the default kernel; 6 / 8 = register-capped variants")
     ap.add_argument("--plain-steps", type=int, default=2)
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--pool-gb", type=float, default=24.0)
@@ -218,7 +220,8 @@ def run_ours(args, dist: Dist):
     max_pairs = max(b.range_pairs for b in steps)
     trees = {}
     for name in ("batched", "plain"):
-        t = mv.gpu_versioned_btree(pool_bytes=pool, tile_width=args.tile_width)
+        t = mv.gpu_versioned_btree(pool_bytes=pool, tile_width=args.tile_width,
+                                   blocks_per_sm=args.blocks_per_sm if name == "batched" else 0)
         t.insert(dev(init), dev(vals))
         t.check_errors()
         trees[name] = t
@@ -340,7 +343,8 @@ def run_ours(args, dist: Dist):
             "initial_keys": args.initial_keys, "batches_per_step": args.batches,
             "batch_size": "lognormal median 16384, sigma 1.5, clipped [1024, 4194304]",
             "mean_ops_per_step": int(mean_ops), "mode": "persistent launch, device work queue",
-            "tile_width": args.tile_width, "parallelism": f"replicas x{dist.world}",
+            "tile_width": args.tile_width, "blocks_per_sm": args.blocks_per_sm,
+            "parallelism": f"replicas x{dist.world}",
             "l2": "inputs larger than L2 (tree of %d nodes = %.1f GB; ops %.0f MB per step)" % (
                 rep["nodes_allocated"], rep["nodes_allocated"] * 128 / 1e9, mean_ops * 24 / 1e6),
             "tree_height": rep["height"], "workload_gen_s": round(gen_s, 1),

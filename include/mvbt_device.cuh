@@ -1289,8 +1289,8 @@ struct batch_sched {
   const uint32_t* params;        // [0] num_batches, [1] snapshot of batch 0
 };
 
-constexpr uint32_t kWriteClaim = 2;
-constexpr uint32_t kReadClaim  = 8;
+constexpr uint32_t kWriteClaim = 1;  // writes per tile per claim
+constexpr uint32_t kReadClaim  = 4;  // reads per tile per claim
 
 // Largest b in [lo, nb) with pre[b] <= x (pre is non-decreasing), starting from the hint lo.
 MVBT_DEV uint32_t batch_of_ordinal(const uint64_t* pre, uint32_t nb, uint64_t x, uint32_t lo) {
@@ -1339,75 +1339,83 @@ MVBT_DEV bool wait_batch_ready(const device_tree& T, const batch_sched& sc, uint
   }
 }
 
-// Worker loop of one tile in the persistent batched launch.
-template <int W, class Tile>
+// Worker loop of one warp in the persistent batched launch. The warp claims consecutive claim
+// positions and hands them to its tiles interleaved (tile j takes every (32/W)-th position), and
+// the claim order inside a batch is writes | finds | ranges, so the tiles of a warp run the same
+// kind of op side by side and their instructions issue together.
+template <int W, class Warp, class Tile>
 MVBT_DEV void batched_worker(const device_tree& T, const batch_view& B, const batch_sched& sc,
-                             const Tile& t) {
-  const uint32_t nb = ld_relaxed_u32(sc.params + 0);
-  const uint32_t S0 = ld_relaxed_u32(sc.params + 1);
+                             const Warp& warp, const Tile& t) {
+  constexpr uint32_t kTiles = 32 / W;
+  const uint32_t tid = warp.thread_rank() / W;
+  const uint32_t nb  = ld_relaxed_u32(sc.params + 0);
+  const uint32_t S0  = ld_relaxed_u32(sc.params + 1);
   const uint64_t TW = sc.wpre[nb], TR = sc.rpre[nb];
   uint32_t wb = 0, rb = 0;  // batch hints for the two queues
   unsigned long long idle_since = 0;
   for (uint32_t spin = 0;;) {
+    warp.sync();
     uint32_t d = 0;
     unsigned long long g = 0, r = 0;
-    if (t.thread_rank() == 0) {
+    if (warp.thread_rank() == 0) {
       d = ld_relaxed_u32(sc.done_batches);
       g = ld_relaxed_u64(sc.wcursor);
       r = ld_relaxed_u64(sc.rcursor);
     }
-    d = t.shfl(d, 0);
-    g = t.shfl(g, 0);
-    r = t.shfl(r, 0);
+    d = warp.shfl(d, 0);
+    g = warp.shfl(g, 0);
+    r = warp.shfl(r, 0);
     if (g >= TW && r >= TR) break;
     __threadfence();  // the batches counted in d are finished: see their writes
-    t.sync();
+    warp.sync();
     bool did = false;
     // writes first: they gate every later batch
     if (g < TW) {
       wb = batch_of_ordinal(sc.wpre, nb, g, wb);
       if (wb <= d) {
         unsigned long long g0 = 0;
-        if (t.thread_rank() == 0) g0 = atomicAdd(sc.wcursor, (unsigned long long)kWriteClaim);
-        g0 = t.shfl(g0, 0);
-        for (unsigned long long x = g0; x < g0 + kWriteClaim && x < TW; ++x) {
-          wb = batch_of_ordinal(sc.wpre, nb, x, wb);
-          if (wb > d) {
-            if (!wait_batch_ready(T, sc, nb, wb, t)) {
-              if (t.thread_rank() == 0) T.set_error(kErrSpinLimit, 14);
-            }
-            d = wb;
+        if (warp.thread_rank() == 0) g0 = atomicAdd(sc.wcursor, (unsigned long long)(kTiles * kWriteClaim));
+        g0 = warp.shfl(g0, 0);
+        did = g0 < TW;
+        uint32_t b = wb, dd = d;
+        for (uint32_t k = 0; k < kWriteClaim; ++k) {
+          const unsigned long long x = g0 + k * kTiles + tid;
+          if (x >= TW) break;
+          b = batch_of_ordinal(sc.wpre, nb, x, b);
+          if (b > dd) {
+            if (!wait_batch_ready(T, sc, nb, b, t) && t.thread_rank() == 0) T.set_error(kErrSpinLimit, 14);
+            dd = b;
           }
-          const uint32_t i = sc.perm[sc.batch_off[wb] + (x - sc.wpre[wb])];
-          run_batch_op<W>(T, B, i, S0 + wb, S0 + wb + 1, t);
+          const uint32_t i = sc.perm[sc.batch_off[b] + (x - sc.wpre[b])];
+          run_batch_op<W>(T, B, i, S0 + b, S0 + b + 1, t);
           __threadfence();
           t.sync();
           if (t.thread_rank() == 0) {
-            uint32_t c = atomicAdd(&sc.writes_done[wb], 1u) + 1u;
-            if (c == sc.n_writes[wb]) advance_done(sc, nb);
+            uint32_t c = atomicAdd(&sc.writes_done[b], 1u) + 1u;
+            if (c == sc.n_writes[b]) advance_done(sc, nb);
           }
         }
-        did = g0 < TW;
       }
     }
     if (!did && r < TR) {
       rb = batch_of_ordinal(sc.rpre, nb, r, rb);
       if (rb <= d) {
         unsigned long long r0 = 0;
-        if (t.thread_rank() == 0) r0 = atomicAdd(sc.rcursor, (unsigned long long)kReadClaim);
-        r0 = t.shfl(r0, 0);
-        for (unsigned long long x = r0; x < r0 + kReadClaim && x < TR; ++x) {
-          rb = batch_of_ordinal(sc.rpre, nb, x, rb);
-          if (rb > d) {
-            if (!wait_batch_ready(T, sc, nb, rb, t)) {
-              if (t.thread_rank() == 0) T.set_error(kErrSpinLimit, 14);
-            }
-            d = rb;
-          }
-          const uint32_t i = sc.perm[sc.batch_off[rb] + sc.n_writes[rb] + (x - sc.rpre[rb])];
-          run_batch_op<W>(T, B, i, S0 + rb, S0 + rb + 1, t);
-        }
+        if (warp.thread_rank() == 0) r0 = atomicAdd(sc.rcursor, (unsigned long long)(kTiles * kReadClaim));
+        r0 = warp.shfl(r0, 0);
         did = r0 < TR;
+        uint32_t b = rb, dd = d;
+        for (uint32_t k = 0; k < kReadClaim; ++k) {
+          const unsigned long long x = r0 + k * kTiles + tid;
+          if (x >= TR) break;
+          b = batch_of_ordinal(sc.rpre, nb, x, b);
+          if (b > dd) {
+            if (!wait_batch_ready(T, sc, nb, b, t) && t.thread_rank() == 0) T.set_error(kErrSpinLimit, 14);
+            dd = b;
+          }
+          const uint32_t i = sc.perm[sc.batch_off[b] + sc.n_writes[b] + (x - sc.rpre[b])];
+          run_batch_op<W>(T, B, i, S0 + b, S0 + b + 1, t);
+        }
       }
     }
     if (did) {
@@ -1416,10 +1424,10 @@ MVBT_DEV void batched_worker(const device_tree& T, const batch_view& B, const ba
       continue;
     }
     // nothing runnable yet: help advance done_batches, then back off (bounded)
-    if (t.thread_rank() == 0) advance_done(sc, nb);
+    if (warp.thread_rank() == 0) advance_done(sc, nb);
     if (idle_since == 0) idle_since = global_ns();
     if (global_ns() - idle_since > T.ctl->wait_ns) {
-      if (t.thread_rank() == 0) T.set_error(kErrSpinLimit, 14);
+      if (warp.thread_rank() == 0) T.set_error(kErrSpinLimit, 14);
       break;
     }
     __nanosleep(spin < 8 ? 256 : 2048);

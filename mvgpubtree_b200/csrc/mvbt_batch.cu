@@ -32,7 +32,7 @@ struct mvbt_batch_plan {
   uint64_t* d_batch_off;  // [max_batches + 1]
   uint32_t* d_params;     // [0] num_batches, [1] snapshot of batch 0
   uint32_t* d_perm;       // [max_ops]
-  uint32_t* d_counts;     // n_writes | writes_done | write fill | read fill (each [max_batches]),
+  uint32_t* d_counts;     // n_writes | n_finds | writes_done | fill (3 classes) (each [max_batches]),
                           // then done_batches
   uint64_t* d_pre;        // write-ordinal prefix [max_batches + 1] | read-ordinal prefix [...]
   unsigned long long* d_cursor;  // write cursor, read cursor
@@ -76,9 +76,15 @@ __device__ __forceinline__ uint32_t batch_of(const uint64_t* off, uint32_t nb, u
   return lo;
 }
 
-// Pass 1: writes per batch (warp-aggregated atomics).
+// Op class in the claim order of a batch: writes | finds | ranges.
+__device__ __forceinline__ uint32_t op_class(uint32_t type) {
+  return mvbt::is_write_op(type) ? 0u : (type == mvbt::kOpFind ? 1u : 2u);
+}
+
+// Pass 1: writes and finds per batch (warp-aggregated atomics).
 __global__ void k_count_writes(const uint32_t* __restrict__ type, const uint64_t* __restrict__ off,
-                               const uint32_t* __restrict__ params, uint32_t* n_writes) {
+                               const uint32_t* __restrict__ params, uint32_t* n_writes,
+                               uint32_t* n_finds) {
   const uint32_t nb    = params[0];
   const uint64_t total = off[nb];
   const uint32_t lane  = threadIdx.x & 31;
@@ -86,20 +92,22 @@ __global__ void k_count_writes(const uint32_t* __restrict__ type, const uint64_t
   for (uint64_t base = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x - lane); base < total;
        base += warps * 32) {
     const uint64_t i   = base + lane;
-    const bool w       = i < total && mvbt::is_write_op(type[i]);
-    const uint32_t act = __ballot_sync(0xFFFFFFFFu, w);
-    if (w) {
+    const uint32_t c   = i < total ? op_class(type[i]) : 2u;
+    const bool counted = c < 2u;
+    const uint32_t act = __ballot_sync(0xFFFFFFFFu, counted);
+    if (counted) {
       const uint32_t b   = batch_of(off, nb, i);
-      const uint32_t grp = __match_any_sync(act, b);
-      if (lane == (uint32_t)(__ffs(grp) - 1)) atomicAdd(&n_writes[b], (uint32_t)__popc(grp));
+      const uint32_t grp = __match_any_sync(act, (b << 1) | c);
+      if (lane == (uint32_t)(__ffs(grp) - 1)) atomicAdd(c == 0 ? &n_writes[b] : &n_finds[b], (uint32_t)__popc(grp));
     }
   }
 }
 
-// Pass 2: claim order with the writes of every batch first.
+// Pass 2: claim order of every batch: writes, then finds, then ranges.
 __global__ void k_place(const uint32_t* __restrict__ type, const uint64_t* __restrict__ off,
                         const uint32_t* __restrict__ params, const uint32_t* __restrict__ n_writes,
-                        uint32_t* wfill, uint32_t* rfill, uint32_t* perm) {
+                        const uint32_t* __restrict__ n_finds, uint32_t* fill, uint32_t mb,
+                        uint32_t* perm) {
   const uint32_t nb    = params[0];
   const uint64_t total = off[nb];
   const uint32_t lane  = threadIdx.x & 31;
@@ -110,17 +118,16 @@ __global__ void k_place(const uint32_t* __restrict__ type, const uint64_t* __res
     const bool live     = i < total;
     const uint32_t livm = __ballot_sync(0xFFFFFFFFu, live);
     if (!live) continue;
-    const bool w        = mvbt::is_write_op(type[i]);
+    const uint32_t c    = op_class(type[i]);
     const uint32_t b    = batch_of(off, nb, i);
-    const uint32_t key  = (b << 1) | (w ? 1u : 0u);
-    const uint32_t grp  = __match_any_sync(livm, key);
+    const uint32_t grp  = __match_any_sync(livm, (b << 2) | c);
     const uint32_t lead = (uint32_t)(__ffs(grp) - 1);
     const uint32_t rank = __popc(grp & ((1u << lane) - 1u));
     uint32_t slot       = 0;
-    if (lane == lead) slot = atomicAdd(w ? &wfill[b] : &rfill[b], (uint32_t)__popc(grp));
+    if (lane == lead) slot = atomicAdd(&fill[c * mb + b], (uint32_t)__popc(grp));
     slot = __shfl_sync(grp, slot, lead);
-    const uint64_t pos = off[b] + (w ? 0u : n_writes[b]) + slot + rank;
-    perm[pos]          = (uint32_t)i;
+    const uint64_t start = c == 0 ? 0u : (c == 1 ? n_writes[b] : n_writes[b] + n_finds[b]);
+    perm[off[b] + start + slot + rank] = (uint32_t)i;
   }
 }
 
@@ -177,10 +184,38 @@ __global__ void k_batch_end(mvbt::control_block* ctl, const uint32_t* params) {
   }
 }
 
+struct launch_ctx {
+  device_tree view;
+  int W, block, sms;
+  uint32_t bps, maxb;
+  mvbt::control_block* ctl;
+};
+
+template <class K>
+unsigned occupancy_grid(const launch_ctx& c, K kernel) {
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, c.block, 0);
+  if (per_sm < 1) per_sm = 1;
+  if (c.bps && (int)c.bps < per_sm) per_sm = (int)c.bps;
+  uint64_t g = (uint64_t)per_sm * c.sms;
+  if (c.maxb) g = std::min<uint64_t>(g, c.maxb);
+  return (unsigned)g;
+}
+
+// MinBlocks > 0 caps registers so that many 256-thread blocks fit on an SM (more traversals in
+// flight, some spills); selected with mvbt_config::blocks_per_sm.
+template <int W, int MinBlocks>
+__global__ void __launch_bounds__(256, MinBlocks) k_batched(device_tree T, batch_view B, batch_sched sc) {
+  auto warp = cg::tiled_partition<32>(cg::this_thread_block());
+  auto tile = cg::tiled_partition<W>(warp);
+  mvbt::batched_worker<W>(T, B, sc, warp, tile);
+}
+
 template <int W>
-__global__ void __launch_bounds__(256) k_batched(device_tree T, batch_view B, batch_sched sc) {
-  auto tile = cg::tiled_partition<W>(cg::this_thread_block());
-  mvbt::batched_worker<W>(T, B, sc, tile);
+void launch_batched(const launch_ctx& c, const batch_view& B, const batch_sched& sc, cudaStream_t s) {
+  if (c.bps >= 8) k_batched<W, 8><<<occupancy_grid(c, k_batched<W, 8>), c.block, 0, s>>>(c.view, B, sc);
+  else if (c.bps >= 6) k_batched<W, 6><<<occupancy_grid(c, k_batched<W, 6>), c.block, 0, s>>>(c.view, B, sc);
+  else k_batched<W, 1><<<occupancy_grid(c, k_batched<W, 1>), c.block, 0, s>>>(c.view, B, sc);
 }
 
 // One batch [begin, end) in one launch: reads at the snapshot in snap_word, writes one epoch later.
@@ -201,41 +236,23 @@ __global__ void k_snapshot_word(mvbt::control_block* ctl, uint32_t* out) {
   }
 }
 
-struct launch_ctx {
-  device_tree view;
-  int W, block, sms;
-  uint32_t bps, maxb;
-  mvbt::control_block* ctl;
-};
-
-template <class K>
-unsigned occupancy_grid(const launch_ctx& c, K kernel) {
-  int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, c.block, 0);
-  if (per_sm < 1) per_sm = 1;
-  if (c.bps && (int)c.bps < per_sm) per_sm = (int)c.bps;
-  uint64_t g = (uint64_t)per_sm * c.sms;
-  if (c.maxb) g = std::min<uint64_t>(g, c.maxb);
-  return (unsigned)g;
-}
-
 int enqueue_persistent(mvbt_batch_plan* p, const launch_ctx& c, const batch_view& B, cudaStream_t s) {
   const uint32_t mb = p->max_batches;
   MVBT_TRY(cudaMemcpyAsync(p->d_batch_off, p->h_batch_off, (mb + 1) * sizeof(uint64_t),
                            cudaMemcpyHostToDevice, s));
   MVBT_TRY(cudaMemcpyAsync(p->d_params, p->h_params, 2 * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
-  MVBT_TRY(cudaMemsetAsync(p->d_counts, 0, (4ull * mb + 4) * sizeof(uint32_t), s));
+  MVBT_TRY(cudaMemsetAsync(p->d_counts, 0, (6ull * mb + 4) * sizeof(uint32_t), s));
   MVBT_TRY(cudaMemsetAsync(p->d_cursor, 0, 2 * sizeof(unsigned long long), s));
   uint32_t* nw    = p->d_counts;
-  uint32_t* wdone = p->d_counts + mb;
-  uint32_t* wfill = p->d_counts + 2 * mb;
-  uint32_t* rfill = p->d_counts + 3 * mb;
-  uint32_t* done  = p->d_counts + 4 * mb;
+  uint32_t* nf    = p->d_counts + mb;
+  uint32_t* wdone = p->d_counts + 2 * mb;
+  uint32_t* fill  = p->d_counts + 3 * mb;
+  uint32_t* done  = p->d_counts + 6 * mb;
   uint64_t* wpre  = p->d_pre;
   uint64_t* rpre  = p->d_pre + (mb + 1);
-  k_count_writes<<<kPrepassBlocks, kPrepassThreads, 0, s>>>(B.type, p->d_batch_off, p->d_params, nw);
-  k_place<<<kPrepassBlocks, kPrepassThreads, 0, s>>>(B.type, p->d_batch_off, p->d_params, nw, wfill,
-                                                     rfill, p->d_perm);
+  k_count_writes<<<kPrepassBlocks, kPrepassThreads, 0, s>>>(B.type, p->d_batch_off, p->d_params, nw, nf);
+  k_place<<<kPrepassBlocks, kPrepassThreads, 0, s>>>(B.type, p->d_batch_off, p->d_params, nw, nf, fill,
+                                                     mb, p->d_perm);
   k_prefix<<<1, 1024, 0, s>>>(p->d_batch_off, p->d_params, nw, wpre, rpre);
   k_batch_begin<<<1, 32, 0, s>>>(c.ctl, p->d_params);
   batch_sched sc;
@@ -251,11 +268,8 @@ int enqueue_persistent(mvbt_batch_plan* p, const launch_ctx& c, const batch_view
   sc.params       = p->d_params;
   const int slot = (int)(p->timed_runs % mvbt_batch_plan::kTimed);
   if (p->timing) cudaEventRecord(p->ev_begin[slot], s);
-  if (c.W == 8) {
-    k_batched<8><<<occupancy_grid(c, k_batched<8>), c.block, 0, s>>>(c.view, B, sc);
-  } else {
-    k_batched<16><<<occupancy_grid(c, k_batched<16>), c.block, 0, s>>>(c.view, B, sc);
-  }
+  if (c.W == 8) launch_batched<8>(c, B, sc, s);
+  else launch_batched<16>(c, B, sc, s);
   if (p->timing) {
     cudaEventRecord(p->ev_end[slot], s);
     ++p->timed_runs;
@@ -288,7 +302,7 @@ int mvbt_batch_plan_create(mvbt_tree* tree, uint64_t max_ops, uint32_t max_batch
   bool ok = cudaMalloc(&p->d_batch_off, (max_batches + 1) * sizeof(uint64_t)) == cudaSuccess &&
             cudaMalloc(&p->d_params, 64) == cudaSuccess &&
             cudaMalloc(&p->d_perm, max_ops * sizeof(uint32_t)) == cudaSuccess &&
-            cudaMalloc(&p->d_counts, (4ull * max_batches + 4) * sizeof(uint32_t)) == cudaSuccess &&
+            cudaMalloc(&p->d_counts, (6ull * max_batches + 4) * sizeof(uint32_t)) == cudaSuccess &&
             cudaMalloc(&p->d_pre, 2ull * (max_batches + 1) * sizeof(uint64_t)) == cudaSuccess &&
             cudaMalloc(&p->d_cursor, 2 * sizeof(unsigned long long)) == cudaSuccess &&
             cudaMallocHost(&p->h_batch_off, (max_batches + 1) * sizeof(uint64_t)) == cudaSuccess &&

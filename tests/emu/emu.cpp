@@ -84,6 +84,29 @@ void run(uint64_t n, int tiles, int W, const std::function<void(uint64_t, const 
   for (auto& x : th) x.join();
 }
 
+// Runs fn(warp, tile) on `warps` emulated warps of 32 threads, each split into tiles of W lanes.
+void run_warps(int warps, int W, const std::function<void(const emu_tile&, const emu_tile&)>& fn) {
+  if (warps < 1) warps = 1;
+  const int tpw = 32 / W;
+  std::vector<std::unique_ptr<tile_shared>> wsh, tsh;
+  for (int w = 0; w < warps; ++w) {
+    wsh.emplace_back(new tile_shared(32));
+    for (int j = 0; j < tpw; ++j) tsh.emplace_back(new tile_shared(W));
+  }
+  std::vector<std::thread> th;
+  for (int w = 0; w < warps; ++w) {
+    for (int l = 0; l < 32; ++l) {
+      th.emplace_back([&, w, l] {
+        mvbt::emu::sm = (uint32_t)w;
+        emu_tile warp{l, 32, wsh[w].get()};
+        emu_tile tile{l % W, W, tsh[w * tpw + l / W].get()};
+        fn(warp, tile);
+      });
+    }
+  }
+  for (auto& x : th) x.join();
+}
+
 }  // namespace
 
 extern "C" {
@@ -209,12 +232,14 @@ void emu_batch_run(void* h, uint32_t nb, const uint64_t* off, const uint32_t* ty
   }
   std::vector<uint32_t> perm(off[nb]), n_writes(nb, 0), writes_done(nb, 0);
   std::vector<uint64_t> wpre(nb + 1, 0), rpre(nb + 1, 0);
-  for (uint32_t b = 0; b < nb; ++b) {
+  for (uint32_t b = 0; b < nb; ++b) {  // claim order: writes | finds | ranges
     uint64_t pos = off[b];
     for (uint64_t i = off[b]; i < off[b + 1]; ++i)
       if (mvbt::is_write_op(type[i])) perm[pos++] = (uint32_t)i, ++n_writes[b];
     for (uint64_t i = off[b]; i < off[b + 1]; ++i)
-      if (!mvbt::is_write_op(type[i])) perm[pos++] = (uint32_t)i;
+      if (type[i] == mvbt::kOpFind) perm[pos++] = (uint32_t)i;
+    for (uint64_t i = off[b]; i < off[b + 1]; ++i)
+      if (type[i] == mvbt::kOpRange) perm[pos++] = (uint32_t)i;
     wpre[b + 1] = wpre[b] + n_writes[b];
     rpre[b + 1] = rpre[b] + (off[b + 1] - off[b]) - n_writes[b];
   }
@@ -223,8 +248,8 @@ void emu_batch_run(void* h, uint32_t nb, const uint64_t* off, const uint32_t* ty
   uint32_t params[2]            = {nb, t->ctl.epoch};
   mvbt::batch_sched sc{off, perm.data(), n_writes.data(), wpre.data(), rpre.data(), writes_done.data(),
                        &done, &cursors[0], &cursors[1], params};
-  EMU_DISPATCH(W, run((uint64_t)tiles, tiles, kW, [&](uint64_t, const emu_tile& tile) {
-    mvbt::batched_worker<kW>(v, B, sc, tile);
+  EMU_DISPATCH(W, run_warps(std::max(1, tiles * kW / 32), kW, [&](const emu_tile& warp, const emu_tile& tile) {
+    mvbt::batched_worker<kW>(v, B, sc, warp, tile);
   }));
   t->ctl.epoch = params[1] + nb;
 }
