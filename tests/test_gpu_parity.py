@@ -276,3 +276,19 @@ def test_spin_limit_gives_up_without_hanging(torch):
     t.find(dev(torch, keys), out)
     got = host(out)
     assert np.all((got == keys) | (got == SENT))
+
+
+def test_cpp_drop_in_caller_runs(torch):
+    """The C++ caller of include/gpu_btree.h (GpuBTree:: class names over the C ABI) gets the
+    reference's known answers: finds and range counts at two snapshots."""
+    import subprocess
+    import sys
+    from pathlib import Path
+    root = Path(__file__).resolve().parent.parent
+    sys.path.insert(0, str(root / "tests" / "cpp"))
+    exe = root / "tests" / "cpp" / "drop_in_example"
+    if not exe.exists():
+        from build import build
+        build()
+    out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0 and "OK" in out.stdout, out.stdout + out.stderr
