@@ -242,6 +242,28 @@ int mvbt_batch_run(mvbt_batch_plan* plan, uint32_t num_batches, const uint64_t* 
 int mvbt_batch_plan_timing(mvbt_batch_plan* plan, int enable);
 int mvbt_batch_plan_kernel_times(mvbt_batch_plan* plan, float* ms, uint32_t max, uint32_t* n);
 
+/* Mixed batches for callers that cannot allocate device memory on their call path: a serving
+ * loop with a latency budget (cudaMalloc / cudaFree can block the device for milliseconds), or a
+ * host application that owns every allocation and gives the library a fixed budget up front.
+ * Same semantics and results as mvbt_batch_run in MVBT_BATCH_PERSISTENT mode, but its scratch
+ * lives in one fixed-size device array inside the library (about 4.3 MB, held by every GPU that
+ * loads the library until the process exits) instead of a batch plan: this call allocates
+ * nothing. It has no counterpart in the reference.
+ * batch_off is a DEVICE array of num_batches + 1 offsets with batch_off[num_batches] == num_ops;
+ * at most MVBT_NOALLOC_MAX_BATCHES batches and MVBT_NOALLOC_MAX_OPS ops (larger requests return
+ * MVBT_ERR_BAD_ARG without touching the GPU). Offsets that do not start at 0, decrease or end
+ * elsewhere than num_ops are rejected on the device: nothing runs and mvbt_check_errors reports
+ * MVBT_ERR_CORRUPT. Every call shares the array (it is cleared where it must start at zero), so
+ * calls that overlap on the GPU (other streams, other threads) race: serialise them. The first
+ * call on a device looks up the array's address; make that first call before any stream
+ * capture. */
+#define MVBT_NOALLOC_MAX_OPS (1u << 20)
+#define MVBT_NOALLOC_MAX_BATCHES 1024u
+int mvbt_batch_run_noalloc(mvbt_tree* tree, uint32_t num_batches, const uint64_t* batch_off,
+                           uint64_t num_ops, const uint32_t* type, const uint32_t* key,
+                           const uint32_t* arg, const uint64_t* out_off, const uint32_t* range_cap,
+                           uint32_t* result, mvbt_pair* range_out, void* stream);
+
 /* Tree kind, tile width and device of a handle. */
 int mvbt_get_info(mvbt_tree* tree, int* kind, int* tile_width, int* device);
 

@@ -16,7 +16,7 @@ from pathlib import Path
 __all__ = [
     "LATEST", "NOT_FOUND", "MVBTError", "lib", "library_path", "gpu_blink_tree",
     "gpu_versioned_btree", "gpu_versioned_blink_tree", "pair_dtype_words", "BatchPlan",
-    "BATCH_PERSISTENT", "BATCH_PER_LAUNCH", "BATCH_GRAPH",
+    "BATCH_PERSISTENT", "BATCH_PER_LAUNCH", "BATCH_GRAPH", "NOALLOC_MAX_OPS", "NOALLOC_MAX_BATCHES",
 ]
 
 LATEST = 0xFFFFFFFF
@@ -90,6 +90,7 @@ _sig("mvbt_batch_plan_timing", ctypes.c_int, _vp, ctypes.c_int)
 _sig("mvbt_batch_plan_kernel_times", ctypes.c_int, _vp, ctypes.POINTER(ctypes.c_float), _u32,
      ctypes.POINTER(_u32))
 _sig("mvbt_stats", ctypes.c_int, _vp, ctypes.POINTER(_u64), _u32)
+_sig("mvbt_batch_run_noalloc", ctypes.c_int, _vp, _u32, _P, _u64, _P, _P, _P, _P, _P, _P, _P, _vp)
 _sig("mvbt_last_error", ctypes.c_char_p)
 _sig("mvbt_status_string", ctypes.c_char_p, ctypes.c_int)
 
@@ -317,6 +318,22 @@ class gpu_versioned_btree(_TreeBase):
         """Scratch for mixed op batches of up to max_ops ops in max_batches batches."""
         return BatchPlan(self, max_ops, max_batches)
 
+    def batch_run_noalloc(self, batch_off, num_ops: int, type, key, arg, out_off, range_cap, result,
+                          range_out, stream=None) -> None:
+        """Mixed batches for callers that cannot allocate device memory on their call path (a
+        latency-bound serving loop, a host that owns every allocation): the scratch lives in a
+        fixed array inside the library, so this call allocates nothing. At most NOALLOC_MAX_OPS
+        ops in NOALLOC_MAX_BATCHES batches; batch_off is a DEVICE tensor of num_batches + 1
+        64-bit offsets. Calls that overlap on the GPU share the array and race."""
+        if not hasattr(batch_off, "numel"):
+            raise TypeError("batch_off must be a device tensor of num_batches + 1 offsets")
+        _check(lib.mvbt_batch_run_noalloc(
+            self._h, int(batch_off.numel()) - 1, _ptr(batch_off, 8, "batch_off"), int(num_ops),
+            _ptr(type, name="type"), _ptr(key, name="key"), _ptr(arg, name="arg"),
+            _ptr(out_off, 8, "out_off"), _ptr(range_cap, name="range_cap"),
+            _ptr(result, name="result"), _ptr(range_out, 8, "range_out"), _stream(stream)),
+            "batch_run_noalloc")
+
     def take_snapshot_async(self, d_out, stream=None) -> None:
         """Stream-ordered snapshot; writes the id to the device word d_out."""
         _check(lib.mvbt_take_snapshot_async(self._h, _stream(stream), _ptr(d_out, name="d_out")),
@@ -324,6 +341,7 @@ class gpu_versioned_btree(_TreeBase):
 
 
 BATCH_PERSISTENT, BATCH_PER_LAUNCH, BATCH_GRAPH = 0, 1, 2
+NOALLOC_MAX_OPS, NOALLOC_MAX_BATCHES = 1 << 20, 1024  # MVBT_NOALLOC_MAX_OPS / _BATCHES
 
 
 class BatchPlan:

@@ -8,6 +8,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 #include <string>
 
 #include "mvbt.h"
@@ -451,3 +452,148 @@ int mvbt_batch_plan_kernel_times(mvbt_batch_plan* p, float* ms, uint32_t max, ui
 }
 
 }  // extern "C"
+
+// ================================================================================================
+// Mixed batches without allocation (mvbt_batch_run_noalloc)
+//
+// Some callers cannot allocate device memory on their call path: a serving loop with a latency
+// budget (cudaMalloc and cudaFree can block the whole device for milliseconds), or a host
+// application that hands the library a fixed memory budget up front and owns every later
+// allocation itself. For them the persistent batched launch can also run with its scratch (claim
+// order, per-batch counters, queue cursors, a checked copy of the batch offsets) in the
+// fixed-size device array below instead of a batch plan. Every GPU that loads the library holds
+// this array (about 4.3 MB) until the process exits. The caller still passes the op, result and
+// output arrays.
+// ================================================================================================
+namespace {
+
+constexpr uint64_t kNoallocPermBytes  = (uint64_t)MVBT_NOALLOC_MAX_OPS * sizeof(uint32_t);
+constexpr uint64_t kNoallocOffBytes   = ((MVBT_NOALLOC_MAX_BATCHES + 1ull) * sizeof(uint64_t) + 255) & ~255ull;
+constexpr uint64_t kNoallocCountBytes = ((6ull * MVBT_NOALLOC_MAX_BATCHES + 4) * sizeof(uint32_t) + 255) & ~255ull;
+constexpr uint64_t kNoallocPreBytes   = (2ull * (MVBT_NOALLOC_MAX_BATCHES + 1) * sizeof(uint64_t) + 255) & ~255ull;
+constexpr uint64_t kNoallocMiscBytes  = 256;  // params (2 words) at 0, the two queue cursors at 64
+constexpr uint64_t kNoallocBytes =
+    kNoallocOffBytes + kNoallocCountBytes + kNoallocPreBytes + kNoallocMiscBytes + kNoallocPermBytes;
+
+// Shared by every call on a device. In host code this name is only a host-side stand-in: the
+// kernels get the device address from noalloc_scratch().
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocBytes];
+
+constexpr int kNoallocMaxDevices = 64;
+void* g_noalloc_ptr[kNoallocMaxDevices] = {};
+std::mutex g_noalloc_mu;
+
+// Device address of g_noalloc_scratch on device `dev` (which must be current). The first call on
+// a device looks it up with cudaGetSymbolAddress; that first call should come before any stream
+// capture.
+int noalloc_scratch(int dev, unsigned char** out) {
+  if (dev < 0 || dev >= kNoallocMaxDevices) return fail(MVBT_ERR_BAD_ARG, "device ordinal out of range");
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* ptr     = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+    if (e != cudaSuccess || !ptr)
+      return fail(MVBT_ERR_CUDA, std::string("cudaGetSymbolAddress(noalloc scratch): ") + cudaGetErrorString(e));
+    g_noalloc_ptr[dev] = ptr;
+  }
+  *out = static_cast<unsigned char*>(g_noalloc_ptr[dev]);
+  return MVBT_OK;
+}
+
+// Checks the caller's device batch offsets (off[0] == 0, non-decreasing, off[nb] == num_ops) and
+// copies them into the scratch; on a mismatch it hands the kernels an empty batch list and records
+// a device error, so no later kernel indexes past the scratch.
+__global__ void k_noalloc_setup(const uint64_t* __restrict__ caller_off, uint32_t nb, uint64_t num_ops,
+                                uint64_t* off, uint32_t* params, mvbt::control_block* ctl) {
+  __shared__ int ok;
+  if (threadIdx.x == 0) ok = (caller_off[0] == 0 && caller_off[nb] == num_ops) ? 1 : 0;
+  __syncthreads();
+  for (uint32_t b = threadIdx.x; b < nb; b += blockDim.x)
+    if (caller_off[b + 1] < caller_off[b]) ok = 0;
+  __syncthreads();
+  for (uint32_t b = threadIdx.x; b <= nb; b += blockDim.x) off[b] = ok ? caller_off[b] : 0;
+  if (threadIdx.x == 0) {
+    params[0] = ok ? nb : 0;
+    params[1] = 0;
+    if (!ok) {
+      atomicOr(&ctl->error, mvbt::kErrCorrupt);
+      atomicAdd(&ctl->err_site[13], 1u);
+    }
+  }
+}
+
+}  // namespace
+
+extern "C" int mvbt_batch_run_noalloc(mvbt_tree* tree, uint32_t num_batches, const uint64_t* batch_off,
+                                      uint64_t num_ops, const uint32_t* type, const uint32_t* key,
+                                      const uint32_t* arg, const uint64_t* out_off,
+                                      const uint32_t* range_cap, uint32_t* result,
+                                      mvbt_pair* range_out, void* stream) {
+  if (!tree || !batch_off || (num_ops && (!type || !key || !arg || !result)))
+    return fail(MVBT_ERR_BAD_ARG, "null argument");
+  if (num_batches > MVBT_NOALLOC_MAX_BATCHES)
+    return fail(MVBT_ERR_BAD_ARG, "mvbt_batch_run_noalloc: more than MVBT_NOALLOC_MAX_BATCHES batches");
+  if (num_ops > MVBT_NOALLOC_MAX_OPS)
+    return fail(MVBT_ERR_BAD_ARG, "mvbt_batch_run_noalloc: more than MVBT_NOALLOC_MAX_OPS ops");
+  if (num_batches == 0 || num_ops == 0) return MVBT_OK;
+  launch_ctx c;
+  void* ctl;
+  int st = mvbt_internal_view(tree, &c.view, &c.W, &c.block, &c.sms, &c.bps, &c.maxb, &ctl);
+  if (st) return st;
+  if (!c.view.versioned) return fail(MVBT_ERR_NOT_SUPPORTED, "mixed batches need a versioned tree");
+  c.ctl = static_cast<mvbt::control_block*>(ctl);
+  int dev = 0;
+  MVBT_TRY(cudaGetDevice(&dev));
+  unsigned char* base = nullptr;
+  st = noalloc_scratch(dev, &base);
+  if (st) return st;
+  constexpr uint32_t mb        = MVBT_NOALLOC_MAX_BATCHES;
+  uint64_t* off                = reinterpret_cast<uint64_t*>(base);
+  uint32_t* counts             = reinterpret_cast<uint32_t*>(base + kNoallocOffBytes);
+  uint64_t* pre                = reinterpret_cast<uint64_t*>(base + kNoallocOffBytes + kNoallocCountBytes);
+  unsigned char* misc          = base + kNoallocOffBytes + kNoallocCountBytes + kNoallocPreBytes;
+  uint32_t* params             = reinterpret_cast<uint32_t*>(misc);
+  unsigned long long* cursor   = reinterpret_cast<unsigned long long*>(misc + 64);
+  uint32_t* perm               = reinterpret_cast<uint32_t*>(misc + kNoallocMiscBytes);
+  batch_view B;
+  B.type      = type;
+  B.key       = key;
+  B.arg       = arg;
+  B.out_off   = out_off;
+  B.cap       = range_cap;
+  B.result    = result;
+  B.range_out = reinterpret_cast<uint2*>(range_out);
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  // the array keeps the previous call's contents: counters and cursors start from zero again
+  MVBT_TRY(cudaMemsetAsync(counts, 0, (6ull * mb + 4) * sizeof(uint32_t), s));
+  MVBT_TRY(cudaMemsetAsync(cursor, 0, 2 * sizeof(unsigned long long), s));
+  k_noalloc_setup<<<1, 256, 0, s>>>(batch_off, num_batches, num_ops, off, params, c.ctl);
+  uint32_t* nw    = counts;
+  uint32_t* nf    = counts + mb;
+  uint32_t* wdone = counts + 2 * mb;
+  uint32_t* fill  = counts + 3 * mb;
+  uint32_t* done  = counts + 6 * mb;
+  uint64_t* wpre  = pre;
+  uint64_t* rpre  = pre + (mb + 1);
+  k_count_writes<<<kPrepassBlocks, kPrepassThreads, 0, s>>>(type, off, params, nw, nf);
+  k_place<<<kPrepassBlocks, kPrepassThreads, 0, s>>>(type, off, params, nw, nf, fill, mb, perm);
+  k_prefix<<<1, 1024, 0, s>>>(off, params, nw, wpre, rpre);
+  k_batch_begin<<<1, 32, 0, s>>>(c.ctl, params);
+  batch_sched sc;
+  sc.batch_off    = off;
+  sc.perm         = perm;
+  sc.n_writes     = nw;
+  sc.wpre         = wpre;
+  sc.rpre         = rpre;
+  sc.writes_done  = wdone;
+  sc.done_batches = done;
+  sc.wcursor      = cursor;
+  sc.rcursor      = cursor + 1;
+  sc.params       = params;
+  if (c.W == 8) launch_batched<8>(c, B, sc, s);
+  else launch_batched<16>(c, B, sc, s);
+  k_batch_end<<<1, 32, 0, s>>>(c.ctl, params);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(MVBT_ERR_CUDA, std::string("batched launch (noalloc): ") + cudaGetErrorString(e));
+  return MVBT_OK;
+}
