@@ -20,11 +20,11 @@
 //   pairs 0..12  {key, value}  leaf: key/value, interior: {separator, child index}; sorted by key,
 //                              unused pairs are {0xFFFFFFFF, 0xFFFFFFFF}
 //   pair 13      {low fence, mod}     low fence = smallest key the node may hold (fixed for the
-//                                     node's life); mod = modification count, bumped and
-//                                     published before every change
+//                                     node's life); mod = bit31 lock | bits 0..30 modification
+//                                     count, bumped by the release that follows a change
 //   pair 14      {high key, link}     high key = exclusive upper fence (0xFFFFFFFF on the
-//                                     rightmost node of a level); link = bit31 lock |
-//                                     bits 0..27 right-sibling index (0x0FFFFFFF = none)
+//                                     rightmost node of a level); link = bits 0..27 right-sibling
+//                                     index (0x0FFFFFFF = none)
 //   pair 15      {ts, older|level}    ts = epoch of this version; bits 28..31 level (0 = leaf),
 //                                     bits 0..27 index of the next older version (none = 0x0FFFFFFF)
 // A tile of W threads (W = 8 or 16) holds one node in registers: lane l owns pairs
@@ -35,11 +35,13 @@
 // writer stores it can mix two versions, even inside one lane. Every visit therefore checks
 // low <= key (a mixed parent can route one child too far right; the visit then restarts from the
 // anchor) and key < high (too far left: follow the right link), and a reader that uses the data of
-// a leaf re-reads its header after a fence (see recheck_version / leaf_changed).
+// a leaf validates it (see recheck_version / read_leaf_latest).
 //
 // Concurrency protocol (B-link, Lehman-Yao style):
 //   * readers never lock; a reader whose key is >= a node's high key follows the right link;
-//   * a writer locks one leaf (atomicOr on the lock bit, bounded spin with __nanosleep backoff),
+//   * a writer locks one leaf (atomicOr on the lock bit of the mod word, bounded spin with
+//     __nanosleep backoff; the release that follows a change clears the bit and bumps the count
+//     in one exchange, so the mod word is a sequence lock for readers of the newest state),
 //     moves right under lock coupling, and applies its change; a full node splits into itself
 //     and a new right sibling (right written first, then left, each followed by a fence), then
 //     the writer releases the node and inserts the separator into the parent recorded on its
@@ -122,7 +124,9 @@ constexpr uint32_t kNotFound  = 0xFFFFFFFFu;
 constexpr uint32_t kLatest    = 0xFFFFFFFFu;  // read the newest version
 constexpr uint32_t kNone      = 0x0FFFFFFFu;  // "no node" in 28-bit index fields
 constexpr uint32_t kIndexMask = 0x0FFFFFFFu;
-constexpr uint32_t kLockBit   = 0x80000000u;
+constexpr uint32_t kLockBit   = 0x80000000u;  // in the mod word (node word 27)
+constexpr uint32_t kCountMask = 0x7FFFFFFFu;  // modification count bits of the mod word
+constexpr int kModWord        = 27;
 constexpr uint32_t kAnchor    = 0;  // fixed entry node: one entry {0 -> top}, level = top + 1
 constexpr uint32_t kFirstLeaf = 1;  // the initial leaf (holds the tombstone {0, 0})
 constexpr int kMaxLevels      = 16;
@@ -632,11 +636,11 @@ struct device_tree {
     return t.shfl(idx, 0);
   }
 
-  // ---- locks on the link word ----
+  // ---- locks on the mod word ----
   template <class Tile>
   MVBT_DEV bool lock(uint32_t idx, const Tile& t) const {
     if (!valid(idx, t)) return false;
-    uint32_t* word               = node_ptr(idx) + 29;
+    uint32_t* word               = node_ptr(idx) + kModWord;
     uint32_t backoff             = 32;
     const uint32_t lim           = ctl->spin_limit;
     const unsigned long long t0  = global_ns();
@@ -664,20 +668,31 @@ struct device_tree {
     if (t.thread_rank() == 0) set_error(kErrSpinLimit, 2);
     return false;
   }
+  // Releases a node this tile locked and left unchanged (the count stays).
   template <class Tile>
   MVBT_DEV void unlock(uint32_t idx, const Tile& t) const {
     __threadfence();
     t.sync();
-    if (t.thread_rank() == 0) atomicAnd(node_ptr(idx) + 29, ~kLockBit);
+    if (t.thread_rank() == 0) atomicAnd(node_ptr(idx) + kModWord, ~kLockBit);
+  }
+  // Releases a node this tile locked and changed: after every lane's stores are ordered (fence +
+  // warp barrier), one exchange clears the lock bit and bumps the count. h.mod is the mod word
+  // read under the lock; while the lock is held only failing lock attempts (atomicOr of a bit
+  // that is already set) touch the word, so the exchange loses nothing.
+  template <class Tile>
+  MVBT_DEV void release(uint32_t idx, const header& h, const Tile& t) const {
+    __threadfence();
+    t.sync();
+    if (t.thread_rank() == 0)
+      atomicExch(node_ptr(idx) + kModWord, ((h.mod & kCountMask) + 1u) & kCountMask);
   }
 
   // ---- versioning ----
   // Makes the version visible to older snapshots immutable before node idx (locked, content n)
-  // is changed in epoch E: copies n to a fresh node and publishes {ts = E, older = copy}.
-  // Every change of a node first bumps and publishes its modification count (and, on a versioned
-  // tree, the first change in epoch E copies the node to a fresh node O and publishes
-  // {ts = E, older = O} with it), then fences, so a concurrent reader that re-reads the header
-  // after reading the data sees that something changed.
+  // is changed in epoch E. On a versioned tree the first change in epoch E copies the node to a
+  // fresh node O and publishes {ts = E, older = O} before any data changes, so a snapshot reader
+  // that re-reads ts after reading the data sees that it must use O. Readers of the newest state
+  // need nothing here: the lock bit and the count bumped by release() cover them.
   template <int W, class Tile>
   MVBT_DEV bool prepare_write(uint32_t idx, node_regs<W>& n, header& h, uint32_t E, const Tile& t) const {
     if (versioned && h.ts != E) {
@@ -685,18 +700,17 @@ struct device_tree {
       if (copy == kNone) return false;
       node_regs<W> c = n;
       header hc      = h;
-      hc.link &= ~kLockBit;
+      hc.mod &= kCountMask;  // the copy is never locked
       set_header<W>(c, hc, t);
       store<W>(copy, c, t);
       publish_fence(t);
       h.ts = E;
       h.ol = (h.ol & ~kIndexMask) | copy;
+      set_header<W>(n, h, t);
+      store_header<W>(idx, n, t);
+      publish_fence(t);
       if (t.thread_rank() == 0) atomicAdd(&ctl->stat_cow, 1ull);
     }
-    h.mod += 1;
-    set_header<W>(n, h, t);
-    store_header<W>(idx, n, t);
-    publish_fence(t);
     return true;
   }
 
@@ -725,15 +739,35 @@ struct device_tree {
   // ts <= snapshot re-reads the header after a fence. A writer publishes {ts = E, older = copy}
   // before it changes the data, so if any lane saw changed data the re-read shows ts > snapshot:
   // the reader then returns the index of the immutable copy (else kNone: the data is consistent).
-  // For readers of the newest state: true if the modification count of leaf idx is no longer
-  // `seen` (a writer changed it while it was being read).
-  template <class Tile>
-  MVBT_DEV bool leaf_changed(uint32_t idx, uint32_t seen, const Tile& t) const {
-    __threadfence();
-    t.sync();
-    uint32_t now = 0;
-    if (t.thread_rank() == 0) now = ld_relaxed_u32(node_ptr(idx) + 27);
-    return t.shfl(now, 0) != seen;
+  // Reads leaf idx for a reader of the newest state while writers may run: a sequence lock on
+  // the mod word (lock bit | count). A writer holds the lock bit while it changes a reachable
+  // leaf and clears it with a bumped count in one exchange after its stores, so the data is
+  // consistent when the mod word is unlocked in a read ordered before the data (fence) and
+  // unchanged in a re-read ordered after it (fence). Lock and count share one word on purpose:
+  // two words read separately could show the state before a writer's lock in one and after its
+  // change in the other. Each lane reads the word itself, so its own fences order it around its
+  // own share of the node; the read counts only if it held in every lane. Bounded: gives up
+  // after the wait limit (kErrSpinLimit) and returns false.
+  template <int W, class Tile>
+  MVBT_DEV bool read_leaf_latest(uint32_t idx, node_regs<W>& n, const Tile& t) const {
+    const uint32_t* p             = node_ptr(idx);
+    const unsigned long long t0   = global_ns();
+    const unsigned long long lim  = ctl->wait_ns;
+    uint32_t backoff              = 32;
+    for (;;) {
+      const uint32_t mod0 = ld_relaxed_u32(p + kModWord);
+      __threadfence();
+      ld_lane<W>(p + t.thread_rank() * (32 / W), n, true);
+      __threadfence();
+      const uint32_t mod1 = ld_relaxed_u32(p + kModWord);
+      const bool torn     = (mod0 & kLockBit) != 0 || mod0 != mod1;
+      if (t.ballot(torn) == 0) return true;
+      if (global_ns() - t0 > lim) break;
+      __nanosleep(backoff);
+      backoff = backoff < 1024 ? backoff * 2 : 1024;
+    }
+    if (t.thread_rank() == 0) set_error(kErrSpinLimit, 2);
+    return false;
   }
 
   template <class Tile>
@@ -754,23 +788,32 @@ struct device_tree {
   template <int W, class Tile>
   MVBT_DEV uint32_t cooperative_find(uint32_t key, const Tile& t, uint32_t ts = kLatest,
                                      bool concurrent = false) const {
-    const bool snap = versioned && ts != kLatest;
-    uint32_t idx    = kAnchor;
-    bool via_older  = false;  // idx was reached through an older-version pointer
+    const bool snap   = versioned && ts != kLatest;
+    const bool seqlk  = !snap && concurrent;  // newest state under writers: read leaves locked-free
+    uint32_t idx      = kAnchor;
+    bool via_older    = false;  // idx was reached through an older-version pointer
+    bool leaf_next    = false;  // idx is a leaf (child of a level-1 node, or a leaf's sibling)
     node_regs<W> n;
     for (uint32_t step = 0; step < kMaxSteps; ++step) {
       if (!valid(idx, t)) return kNotFound;
-      load<W>(idx, n, concurrent, t);
+      const bool stable = seqlk && leaf_next;
+      if (stable) {
+        if (!read_leaf_latest<W>(idx, n, t)) return kNotFound;
+      } else {
+        load<W>(idx, n, concurrent, t);
+      }
       header h  = get_header<W>(n, t);
       bool copy = via_older;
       via_older = false;
       if (snap && !to_version<W>(idx, n, h, ts, concurrent, copy, t)) return kNotFound;
       if (key < h.low) {  // routed too far right by a torn read upstream: start over
-        idx = kAnchor;
+        idx       = kAnchor;
+        leaf_next = false;
         continue;
       }
       if (key >= h.high && h.sibling() != kNone) {
-        idx = h.sibling();
+        idx       = h.sibling();
+        leaf_next = h.is_leaf();
         continue;
       }
       if (h.is_leaf()) {
@@ -781,13 +824,18 @@ struct device_tree {
             via_older = true;
             continue;
           }
-        } else if (!snap && concurrent && leaf_changed(idx, h.mod, t)) {
-          continue;  // a writer changed the leaf while it was read: read it again
+        } else if (seqlk && !stable) {
+          leaf_next = true;  // reached without knowing it was a leaf: read it again, consistently
+          continue;
         }
         return leaf_value<W>(n, key, t);
       }
-      idx = child_for<W>(n, key, t);
-      if (idx == kNone) idx = kAnchor;
+      leaf_next = h.level() == 1;
+      idx       = child_for<W>(n, key, t);
+      if (idx == kNone) {
+        idx       = kAnchor;
+        leaf_next = false;
+      }
     }
     if (t.thread_rank() == 0) set_error(kErrStepLimit, 4);
     return kNotFound;
@@ -802,9 +850,11 @@ struct device_tree {
                                             uint2* out, uint32_t cap, bool concurrent = false) const {
     constexpr int P = 16 / W;
     if (hi <= lo) return 0;
-    const bool snap = versioned && ts != kLatest;
-    uint32_t idx    = kAnchor;
-    bool via_older  = false;
+    const bool snap  = versioned && ts != kLatest;
+    const bool seqlk = !snap && concurrent;  // newest state under writers (read_leaf_latest)
+    uint32_t idx     = kAnchor;
+    bool via_older   = false;
+    bool leaf_next   = false;
     node_regs<W> n;
     header h;
     // descend to the leaf that holds lo and settle on a consistent version of it
@@ -814,17 +864,24 @@ struct device_tree {
         return 0;
       }
       if (!valid(idx, t)) return 0;
-      load<W>(idx, n, concurrent, t);
+      const bool stable = seqlk && leaf_next;
+      if (stable) {
+        if (!read_leaf_latest<W>(idx, n, t)) return 0;
+      } else {
+        load<W>(idx, n, concurrent, t);
+      }
       h         = get_header<W>(n, t);
       bool copy = via_older;
       via_older = false;
       if (snap && !to_version<W>(idx, n, h, ts, concurrent, copy, t)) return 0;
       if (lo < h.low) {
-        idx = kAnchor;
+        idx       = kAnchor;
+        leaf_next = false;
         continue;
       }
       if (lo >= h.high && h.sibling() != kNone) {
-        idx = h.sibling();
+        idx       = h.sibling();
+        leaf_next = h.is_leaf();
         continue;
       }
       if (h.is_leaf()) {
@@ -835,13 +892,18 @@ struct device_tree {
             via_older = true;
             continue;
           }
-        } else if (!snap && concurrent && leaf_changed(idx, h.mod, t)) {
+        } else if (seqlk && !stable) {
+          leaf_next = true;
           continue;
         }
         break;
       }
-      idx = child_for<W>(n, lo, t);
-      if (idx == kNone) idx = kAnchor;
+      leaf_next = h.level() == 1;
+      idx       = child_for<W>(n, lo, t);
+      if (idx == kNone) {
+        idx       = kAnchor;
+        leaf_next = false;
+      }
     }
     // scan leaves to the right (a sibling chain is never longer than the pool)
     uint32_t count = 0;
@@ -879,7 +941,11 @@ struct device_tree {
       bool settled  = false;
       for (uint32_t tries = 0; tries < kMaxSteps && !settled; ++tries) {
         if (!valid(idx, t)) return count;
-        load<W>(idx, n, concurrent, t);
+        if (seqlk) {
+          if (!read_leaf_latest<W>(idx, n, t)) return count;
+        } else {
+          load<W>(idx, n, concurrent, t);
+        }
         h         = get_header<W>(n, t);
         bool copy = via_older;
         via_older = false;
@@ -891,8 +957,6 @@ struct device_tree {
             via_older = true;
             continue;
           }
-        } else if (!snap && concurrent && leaf_changed(idx, h.mod, t)) {
-          continue;
         }
         settled = true;
       }
@@ -1058,14 +1122,14 @@ struct device_tree {
     uint32_t rmin = t.shfl(right.k[0], 0);
     header hr = make_header(rmin, 0u, h.high, h.sibling(), ts,
                             (h.level() << 28) | (versioned ? h.older() : kNone));
-    header hl = make_header(h.low, h.mod, rmin, r | kLockBit, h.ts, h.ol);
+    header hl = make_header(h.low, h.mod, rmin, r, h.ts, h.ol);
     set_header<W>(right, hr, t);
     set_header<W>(left, hl, t);
     store<W>(r, right, t);
     publish_fence(t);
     store<W>(idx, left, t);
     if (t.thread_rank() == 0) atomicAdd(&ctl->stat_split, 1ull);
-    unlock(idx, t);
+    release(idx, h, t);
     sep_key   = rmin;
     sep_child = r;
     return true;
@@ -1102,7 +1166,7 @@ struct device_tree {
     set_header<W>(n, h, t);
     store<W>(kAnchor, n, t);
     if (t.thread_rank() == 0) atomicAdd(&ctl->stat_split, 1ull);
-    unlock(kAnchor, t);
+    release(kAnchor, h, t);
     return true;
   }
 
@@ -1129,7 +1193,7 @@ struct device_tree {
         for (int j = 0; j < 16 / W; ++j)
           if (pair_index<W>(t, j) == pos) n.v[j] = value;
         store<W>(leaf, n, t);
-        unlock(leaf, t);
+        release(leaf, h, t);
         return true;
       }
       if (!prepare_write<W>(leaf, n, h, E, t)) {
@@ -1142,7 +1206,7 @@ struct device_tree {
         node_regs<W> out;
         build_from_merged<W>(n, ipos, key, value, 0, nvalid + 1, out, t);
         store<W>(leaf, out, t);
-        unlock(leaf, t);
+        release(leaf, h, t);
         return true;
       }
       // full leaf: split, then push separators up
@@ -1174,7 +1238,7 @@ struct device_tree {
           node_regs<W> out;
           build_from_merged<W>(n, ipos, sep_key, sep_child, 0, nvalid + 1, out, t);
           store<W>(p, out, t);
-          unlock(p, t);
+          release(p, h, t);
           return true;
         }
         uint32_t k2 = sep_key, c2 = sep_child;
@@ -1207,7 +1271,7 @@ struct device_tree {
     }
     remove_at<W>(n, pos, t);
     store<W>(leaf, n, t);
-    unlock(leaf, t);
+    release(leaf, h, t);
     return true;
   }
 

@@ -31,7 +31,7 @@ struct host_node {
   uint32_t val(int p) const { return w[2 * p + 1]; }
   uint32_t low() const { return w[26]; }
   uint32_t high() const { return w[28]; }
-  uint32_t link() const { return w[29]; }
+  uint32_t mod() const { return w[27]; }  // bit31 lock | modification count
   uint32_t ts() const { return w[30]; }
   uint32_t level() const { return w[31] >> 28; }
   uint32_t older() const { return w[31] & kMask; }
@@ -99,7 +99,7 @@ extern "C" int mvbt_validate_image_detail(const uint32_t* img, uint64_t nn, int 
         ++violations;
         note("stored-low-fence", level, slot, x.low(), low);
       }
-      if (x.link() & kLock) ++rep->locked_nodes;
+      if (x.mod() & kLock) ++rep->locked_nodes;
       uint32_t prev = 0;
       bool have     = false;
       int cnt       = 0;

@@ -28,6 +28,7 @@ def lib():
             "emu_find": (None, [vp, u32p, u32p, u64, u32, i, i]),
             "emu_range": (None, [vp, u32p, u32p, vp, vp, u32, u64, u32, i, i]),
             "emu_insert_range": (None, [vp, u32p, u32p, u64, u32p, u32p, u64, vp, vp, u32, i, i]),
+            "emu_find_erase": (None, [vp, u32p, u32p, u64, u32p, u64, i, i]),
             "emu_validate": (i, [vp, u32, vp]),
             "emu_stats": (None, [vp, np.ctypeslib.ndpointer(dtype=np.uint64, flags="C_CONTIGUOUS")]),
             "emu_batch_run": (None, [vp, u32, np.ctypeslib.ndpointer(dtype=np.uint64, flags="C_CONTIGUOUS"),
@@ -95,6 +96,12 @@ class EmuTree:
         self.L.emu_range(self.h, lo, hi, pairs.ctypes.data, counts.ctypes.data, avg_len, n, ts,
                          self.tiles, self.W)
         return pairs, counts
+
+    def find_erase(self, fk, ek):
+        fk, ek = _u32(fk), _u32(ek)
+        out = np.empty_like(fk)
+        self.L.emu_find_erase(self.h, fk, out, fk.size, ek, ek.size, self.tiles, self.W)
+        return out
 
     def insert_range(self, k, v, lo, hi, avg_len):
         k, v, lo, hi = _u32(k), _u32(v), _u32(lo), _u32(hi)

@@ -212,6 +212,23 @@ void emu_insert_range(void* h, const uint32_t* keys, const uint32_t* vals, uint6
   }));
 }
 
+// One run mixing finds of the newest state and erases (the plain tree's concurrent_find_erase).
+void emu_find_erase(void* h, const uint32_t* fkeys, uint32_t* out, uint64_t n_find,
+                    const uint32_t* ekeys, uint64_t n_erase, int tiles, int W) {
+  auto* t              = static_cast<emu_tree*>(h);
+  auto v               = t->view();
+  const uint64_t total = n_find + n_erase;
+  EMU_DISPATCH(W, run(total, tiles, kW, [&](uint64_t i, const emu_tile& tile) {
+    uint64_t a = (i * n_erase) / total, b = ((i + 1) * n_erase) / total;
+    if (b > a) {
+      v.cooperative_erase<kW>(ekeys[a], tile, 0u);
+    } else {
+      uint32_t r = v.cooperative_find<kW>(fkeys[i - a], tile, mvbt::kLatest, true);
+      if (tile.thread_rank() == 0) out[i - a] = r;
+    }
+  }));
+}
+
 // Mixed batches. mode 0: the persistent worker loop (claim order writes-first per batch, batch b
 // waits for the writes of batch b - 1); mode 1: one snapshot + one run per batch.
 void emu_batch_run(void* h, uint32_t nb, const uint64_t* off, const uint32_t* type, const uint32_t* key,

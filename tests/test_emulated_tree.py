@@ -61,6 +61,32 @@ def test_emulated_concurrent_insert_range_at_launch_snapshot(w):
     assert rep0["violations"] == 0 and rep0["keys"] == n0 + 1
 
 
+@pytest.mark.parametrize("w", [8, 16])
+def test_emulated_find_erase_newest_state(w):
+    """Finds of the newest state running beside erases that shift leaf pairs (the plain tree's
+    concurrent_find_erase): a find returns the key's value, or not-found only for an erased key
+    (include/validation.hpp:106-149 of the reference accepts exactly these)."""
+    from emu import EmuTree
+    from mvgpubtree_b200 import workload as wl
+    import oracle
+    seed, n0 = 21, 6000
+    keys = wl.distinct_keys(seed, 0, n0)
+    vals = wl.values_for(keys, seed)
+    t = EmuTree(False, capacity=1 << 15, tiles=8, W=w)
+    t.insert(keys, vals)
+    er = wl.shuffle(seed + 1, keys)[: n0 // 2]
+    fk = wl.shuffle(seed + 2, keys)
+    got = t.find_erase(fk, er)
+    assert t.errors == 0
+    expect = wl.values_for(fk, seed)
+    erased = np.isin(fk, er)
+    assert np.all((got == expect) | (erased & (got == 0xFFFFFFFF)))
+    m = oracle.MVMap(False)
+    m.insert(keys, vals)
+    m.erase(er)
+    assert np.array_equal(t.find(keys), m.find(keys))
+
+
 def test_emulated_updates_erases_keep_old_snapshots():
     from emu import EmuTree
     from mvgpubtree_b200 import workload as wl

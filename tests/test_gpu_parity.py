@@ -188,6 +188,9 @@ def test_concurrent_find_erase(torch, kind):
     cls = mv.gpu_versioned_btree if kind == "versioned" else mv.gpu_blink_tree
     t = cls(pool_bytes=1 << 30)
     t.insert(dev(torch, keys), dev(torch, vals))
+    before = torch.empty(n0, dtype=torch.int32, device="cuda")
+    t.find(dev(torch, keys), before)
+    assert np.array_equal(host(before), vals), "tree wrong before the concurrent phase"
     er = wl.shuffle(seed + 1, keys)[: n0 // 2]
     fk = wl.shuffle(seed + 2, keys)[: n0 // 2]
     out = torch.empty(len(fk), dtype=torch.int32, device="cuda")
@@ -200,7 +203,14 @@ def test_concurrent_find_erase(torch, kind):
     else:
         # reference acceptance (include/validation.hpp:106-149): found, or the key was erased
         erased = np.isin(fk, er)
-        assert np.all((got == expect) | (erased & (got == SENT)))
+        ok = (got == expect) | (erased & (got == SENT))
+        bad = np.nonzero(~ok)[0]
+        assert bad.size == 0, (
+            f"{bad.size} bad finds: {int(np.sum(~erased[bad] & (got[bad] == SENT)))} live keys not "
+            f"found, {int(np.sum(got[bad] != SENT))} wrong values; first: "
+            + ", ".join(f"key {int(fk[i]):#x} got {int(got[i]):#x} expect {int(expect[i]):#x} "
+                        f"erased {bool(erased[i])}" for i in bad[:4])
+            + f"; stats {t.stats()}")
     out2 = torch.empty(len(keys), dtype=torch.int32, device="cuda")
     t.find(dev(torch, keys), out2)
     m = oracle.MVMap(kind == "versioned")
