@@ -15,9 +15,12 @@ e2e      : Mops/s through the public batch API with host buffers: per step the o
 plain    : the same batches as one snapshot + one launch per batch (the drop-in method).
 roofline : algorithmic bytes of the persistent kernel per launch / its CUDA-event time.
 
-With --impl reference the script times the reference-side CPU implementation of the path (the
-oracle's multiversion ordered map, key-range partitioned over all host cores) on a bounded
-sample of every step of the same workload.
+With --impl reference the script times the reference implementation's own CUDA build
+(oracle/_ref/ref_driver, built by oracle/ref_build.py from the reference's unmodified headers) on
+the same batches through its public host API, one batch at a time (take_snapshot, find(ts),
+range_query(ts), insert, erase), and reports the oracle's multiversion ordered map
+(key-range partitioned over all host cores, bounded sample of every step) as its cpu_baseline.
+Without the reference build it times that CPU map instead.
 """
 from __future__ import annotations
 
@@ -400,30 +403,62 @@ def cpu_oracle_time(init, vals, batches, max_ops: int):
     return cores, build_s, times, ops
 
 
+REF_DRIVER = Path(__file__).resolve().parent / "oracle" / "_ref" / "ref_driver"
+
+
+def reference_build_time(args, W: int, K: int):
+    """The reference implementation's own CUDA build (oracle/_ref/ref_driver, compiled from the
+    reference's unmodified headers) on this workload: same generator, seed and batches, each batch
+    issued through the reference's public host API in its plain form (take_snapshot, find(ts),
+    range_query(ts), insert, erase). Returns its JSON line, or (None, why)."""
+    if not REF_DRIVER.exists():
+        return None, "reference build not present (oracle/ref_build.py builds it where the reference sources are)"
+    cmd = [str(REF_DRIVER), "c4", "--initial", str(args.initial_keys), "--batches", str(args.batches),
+           "--steps", str(K), "--warmup", str(W), "--seed", str(args.seed), "--checksums", "0"]
+    try:
+        out = subprocess.run(cmd, capture_output=True, text=True, timeout=1200)
+    except subprocess.TimeoutExpired:
+        return None, "reference build timed out"
+    if out.returncode != 0:
+        return None, f"reference build failed ({out.returncode}): {out.stderr.strip()[-300:]}"
+    return json.loads(out.stdout.strip().splitlines()[-1]), None
+
+
 def run_reference(args, dist: Dist):
-    """Reference arm: the CPU implementation on the box's host cores (rank 0 only)."""
+    """Reference arm (rank 0 only): the reference implementation's own CUDA build on this B200 and
+    this workload; the oracle port on the host cores is reported beside it as cpu_baseline (and is
+    the arm's value where the reference build is absent)."""
     if dist.rank != 0:
         return None
     W, K = max(3, args.warmup), args.steps
+    ref, why = reference_build_time(args, W, K)
     init, vals, steps, _ = make_workload(args.seed, args.initial_keys, W + K, args.batches)
     cores, build_s, times, ops = cpu_oracle_time(init, vals, steps, args.cpu_sample_ops)
     t = sum(times[W:])
     n = sum(ops[W:])
-    value = n / t / 1e6
+    cpu_value = n / t / 1e6
     sample = (f"first batches of each step up to {args.cpu_sample_ops} ops (mean "
               f"{int(n / K)} ops/step) on the 40M-key map; build {build_s:.1f} s untimed")
+    cpu = {"value": round(cpu_value, 3), "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
+    config = {"workload": "mixed batches on a 40M-key versioned tree, one snapshot per batch "
+                          "(same generator, seed and batches as the GPU arm)",
+              "initial_keys": args.initial_keys, "batches_per_step": args.batches}
+    if ref is not None:
+        value, ms_per_step = ref["mops"], ref["ms"] / K
+        config["implementation"] = ("reference CUDA build (unmodified headers, nvcc sm_100a, its own "
+                                    "flags) through its public host API, one batch at a time: "
+                                    "take_snapshot, find(ts), range_query(ts), insert(in_place), erase")
+        config["ops_timed"] = ref["ops_timed"]
+    else:
+        value, ms_per_step = cpu_value, 1e3 * t / K
+        config["implementation"] = ("oracle multiversion ordered map (std::map per key-range partition, "
+                                    f"one partition per host thread); {why}")
     return {
         "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": UNIT,
-        "n_gpus": dist.world, "steps": K, "warmup": W, "ms_per_step": round(1e3 * t / K, 3),
+        "n_gpus": dist.world, "steps": K, "warmup": W, "ms_per_step": round(ms_per_step, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
-        "data": "synthetic (seeded)",
-        "config": {"workload": "mixed batches on a 40M-key versioned tree, one snapshot per batch "
-                               "(same generator and seed as the GPU arm)",
-                   "initial_keys": args.initial_keys, "batches_per_step": args.batches,
-                   "implementation": "oracle multiversion ordered map (std::map per key-range "
-                                     "partition, one partition per host thread)"},
-        "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": sample},
+        "data": "synthetic (seeded)", "config": config,
+        "cpu_baseline": cpu,
         "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 

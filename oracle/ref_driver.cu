@@ -1,0 +1,423 @@
+// ref_driver.cu -- runs the reference implementation (owensgroup/MVGpuBTree, its unmodified
+// headers) through the reference's own public host API, on workloads from this repository's
+// generator (include/mvbt_workload.h), and prints one JSON line with throughput and checksums of
+// every result. It is test and baseline infrastructure: oracle/ref_build.py compiles it, and only
+// the tests and bench.py's reference arm run it.
+//
+// Modes:
+//   c1 --n N --seed S
+//      Plain B-link tree, GpuBTree::gpu_blink_tree<uint32_t, uint32_t> (reference
+//      include/gpu_blink_tree.hpp:63-67): insert N distinct keys of seed S with values
+//      fmix32(key ^ S), then N finds shuffled from N/2 inserted keys and N - N/2 keys that were
+//      never inserted (include/gpu_blink_tree.hpp:218-236).
+//   c4 --initial N --batches B --steps K --warmup W --seed S [--stride D] [--median M]
+//      [--batch-min A] [--batch-max Z] [--final-chunks C] [--checksums 0|1]
+//      Versioned tree, GpuBTree::gpu_versioned_btree<uint32_t, uint32_t>
+//      (include/gpu_versioned_blink_tree.hpp:71-75), N distinct keys of seed S with values
+//      fmix32(key ^ 0), then W + K steps of B mixed batches each, issued one batch at a time in
+//      the reference's plain form (include/gpu_versioned_blink_tree.hpp:106-216, 297-302):
+//        S_b = take_snapshot(); find(keys, S_b); range_query(lo, hi, S_b); insert(in_place); erase
+//      Reads see the state after every earlier batch; the batch's own writes follow them. Only the
+//      K later steps are timed (CUDA events on the launching stream). With --final-chunks C the
+//      whole key space [1, 2^32 - 1) is read at a final snapshot as C consecutive range queries.
+//
+// Checksums (the tests compute the same sums from this library's outputs): with
+// mix(x) = the SplitMix64 finalizer of x + 0x9E3779B97F4A7C15 and i an op's index in its step,
+//   find  = sum over finds of mix(i << 32 | value)
+//   count = sum over range queries of mix((i << 32 | count) ^ 0xC3A5C85C97CB3127)
+//   pairs = sum over range queries and j < min(count, capacity_i) of
+//           mix(mix((i << 20 | j) ^ 0xB492B66FBE98F273) ^ (key_j << 32 | value_j))
+// all modulo 2^64. The range slot of a batch holds as many pairs as the largest capacity among
+// its queries; the reference writes every hit (it has no bound), so the buffer carries a tail of
+// 1024 * stride pairs, more than any query [lo, lo + L * stride) with L <= 1024 can return.
+#include <gpu_btree.h>
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../include/mvbt_workload.h"
+
+namespace {
+
+using key_t   = uint32_t;
+using value_t = uint32_t;
+using pair_t  = pair_type<key_t, value_t>;
+using vnode_t = GpuBTree::node_type<key_t, value_t, 16>;
+// 2^28 nodes (32 GiB): room for a 40M-key tree and the versions of many steps of batches. The
+// reference's bump allocator does not check its bound (include/device_bump_allocator.hpp:46-54),
+// so the driver refuses workloads that could come near it (kPoolNodes).
+using valloc_t  = device_bump_allocator<vnode_t, (1ull << 28)>;
+using vtree_t   = GpuBTree::gpu_versioned_btree<key_t, value_t, 16, valloc_t>;
+using btree_t   = GpuBTree::gpu_blink_tree<key_t, value_t, 16>;
+constexpr uint64_t kPoolNodes = 1ull << 28;
+
+void check(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) {
+    std::fprintf(stderr, "ref_driver: %s: %s\n", what, cudaGetErrorString(e));
+    std::exit(3);
+  }
+}
+
+uint64_t mix(uint64_t x) {
+  x += 0x9E3779B97F4A7C15ull;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+  return x ^ (x >> 31);
+}
+uint64_t find_term(uint64_t i, uint32_t v) { return mix(i << 32 | v); }
+uint64_t count_term(uint64_t i, uint32_t c) { return mix((i << 32 | c) ^ 0xC3A5C85C97CB3127ull); }
+uint64_t pair_term(uint64_t i, uint64_t j, uint32_t k, uint32_t v) {
+  return mix(mix((i << 20 | j) ^ 0xB492B66FBE98F273ull) ^ ((uint64_t)k << 32 | v));
+}
+
+struct args_t {
+  std::string mode;
+  uint64_t n = 1 << 20, initial = 1 << 20, seed = 1;
+  uint32_t batches = 16, steps = 1, warmup = 0, final_chunks = 0, checksums = 1;
+  uint64_t stride = 0;
+  double median = 0;
+  uint32_t batch_min = 0, batch_max = 0;
+};
+
+args_t parse(int argc, char** argv) {
+  args_t a;
+  if (argc < 2) {
+    std::fprintf(stderr, "usage: ref_driver c1|c4 [--key value]...\n");
+    std::exit(2);
+  }
+  a.mode = argv[1];
+  for (int i = 2; i + 1 < argc; i += 2) {
+    std::string k = argv[i];
+    const char* v = argv[i + 1];
+    if (k == "--n") a.n = std::strtoull(v, nullptr, 10);
+    else if (k == "--initial") a.initial = std::strtoull(v, nullptr, 10);
+    else if (k == "--seed") a.seed = std::strtoull(v, nullptr, 10);
+    else if (k == "--batches") a.batches = (uint32_t)std::strtoul(v, nullptr, 10);
+    else if (k == "--steps") a.steps = (uint32_t)std::strtoul(v, nullptr, 10);
+    else if (k == "--warmup") a.warmup = (uint32_t)std::strtoul(v, nullptr, 10);
+    else if (k == "--final-chunks") a.final_chunks = (uint32_t)std::strtoul(v, nullptr, 10);
+    else if (k == "--checksums") a.checksums = (uint32_t)std::strtoul(v, nullptr, 10);
+    else if (k == "--stride") a.stride = std::strtoull(v, nullptr, 10);
+    else if (k == "--median") a.median = std::strtod(v, nullptr);
+    else if (k == "--batch-min") a.batch_min = (uint32_t)std::strtoul(v, nullptr, 10);
+    else if (k == "--batch-max") a.batch_max = (uint32_t)std::strtoul(v, nullptr, 10);
+    else {
+      std::fprintf(stderr, "ref_driver: unknown option %s\n", k.c_str());
+      std::exit(2);
+    }
+  }
+  return a;
+}
+
+template <class T>
+T* dev_alloc(uint64_t n) {
+  T* p = nullptr;
+  check(cudaMalloc(&p, std::max<uint64_t>(n, 1) * sizeof(T)), "cudaMalloc");
+  return p;
+}
+template <class T>
+T* dev_copy(const std::vector<T>& h) {
+  T* p = dev_alloc<T>(h.size());
+  if (!h.empty()) check(cudaMemcpy(p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice), "upload");
+  return p;
+}
+template <class T>
+std::vector<T> host_copy(const T* d, uint64_t n) {
+  std::vector<T> h(n);
+  if (n) check(cudaMemcpy(h.data(), d, n * sizeof(T), cudaMemcpyDeviceToHost), "download");
+  return h;
+}
+
+float elapsed_ms(cudaEvent_t a, cudaEvent_t b) {
+  float ms = 0;
+  check(cudaEventElapsedTime(&ms, a, b), "cudaEventElapsedTime");
+  return ms;
+}
+
+int run_c1(const args_t& a) {
+  const uint64_t n = a.n;
+  std::vector<uint32_t> keys(n), vals(n), q(n), out(n);
+  mvbt_wl_distinct_keys(a.seed, 0, n, keys.data());
+  mvbt_wl_values(keys.data(), n, (uint32_t)a.seed, vals.data());
+  std::vector<uint32_t> hits(keys);
+  mvbt_wl_shuffle(a.seed + 1, hits.data(), n);
+  const uint64_t nh = n / 2;
+  std::copy(hits.begin(), hits.begin() + nh, q.begin());
+  mvbt_wl_distinct_keys(a.seed, MVBT_MISS_INDEX_BASE, n - nh, q.data() + nh);
+  mvbt_wl_shuffle(a.seed + 2, q.data(), n);
+
+  uint32_t *dk = dev_copy(keys), *dv = dev_copy(vals), *dq = dev_copy(q), *dr = dev_alloc<uint32_t>(n);
+  btree_t tree;
+  cudaEvent_t e0, e1, e2;
+  check(cudaEventCreate(&e0), "event");
+  check(cudaEventCreate(&e1), "event");
+  check(cudaEventCreate(&e2), "event");
+  check(cudaDeviceSynchronize(), "setup");
+  check(cudaEventRecord(e0, 0), "record");
+  tree.insert(dk, dv, (uint32_t)n, 0);
+  check(cudaEventRecord(e1, 0), "record");
+  tree.find(dq, dr, (uint32_t)n, 0, false);
+  check(cudaEventRecord(e2, 0), "record");
+  check(cudaEventSynchronize(e2), "sync");
+  check(cudaGetLastError(), "kernels");
+  const float ins_ms = elapsed_ms(e0, e1), find_ms = elapsed_ms(e1, e2);
+  out = host_copy(dr, n);
+  uint64_t cs = 0;
+  for (uint64_t i = 0; i < n; ++i) cs += find_term(i, out[i]);
+  std::printf(
+      "{\"mode\": \"c1\", \"n\": %llu, \"seed\": %llu, \"insert_ms\": %.4f, \"find_ms\": %.4f, "
+      "\"insert_mops\": %.3f, \"find_mops\": %.3f, \"find_checksum\": %llu}\n",
+      (unsigned long long)n, (unsigned long long)a.seed, ins_ms, find_ms, n / (ins_ms * 1e3), n / (find_ms * 1e3),
+      (unsigned long long)cs);
+  cudaFree(dk);
+  cudaFree(dv);
+  cudaFree(dq);
+  cudaFree(dr);
+  return 0;
+}
+
+// One step of batches split per op kind, in the order the reference's plain form issues them.
+struct step_t {
+  uint32_t nb = 0;
+  std::vector<uint64_t> batch_off;
+  std::vector<uint32_t> type, key, arg, cap;
+  // per batch: [begin, end) in the per-kind arrays, and the range slot size
+  std::vector<uint64_t> f0, r0, i0, e0, p0;
+  std::vector<uint32_t> slot;
+  std::vector<uint32_t> fkeys, lo, hi, ikeys, ivals, ekeys;
+  std::vector<uint64_t> fop, rop;  // op index of each find / range query
+  uint64_t pairs = 0, num_ops = 0;
+};
+
+step_t split(void* gen, uint32_t batches, uint64_t stride) {
+  step_t s;
+  s.nb      = batches;
+  uint64_t range_pairs = 0;
+  s.num_ops = mvbt_wl_mix_generate(gen, batches, &range_pairs);
+  const uint64_t n = s.num_ops;
+  s.batch_off.resize(batches + 1);
+  s.type.resize(n);
+  s.key.resize(n);
+  s.arg.resize(n);
+  s.cap.resize(n);
+  std::vector<uint64_t> out_off(n);
+  mvbt_wl_mix_copy(gen, s.batch_off.data(), s.type.data(), s.key.data(), s.arg.data(), out_off.data(),
+                   s.cap.data());
+  for (uint32_t b = 0; b < batches; ++b) {
+    s.f0.push_back(s.fkeys.size());
+    s.r0.push_back(s.lo.size());
+    s.i0.push_back(s.ikeys.size());
+    s.e0.push_back(s.ekeys.size());
+    s.p0.push_back(s.pairs);
+    uint32_t slot = 8;
+    for (uint64_t i = s.batch_off[b]; i < s.batch_off[b + 1]; ++i) {
+      switch (s.type[i]) {
+        case MVBT_OP_FIND: s.fkeys.push_back(s.key[i]); s.fop.push_back(i); break;
+        case MVBT_OP_RANGE:
+          s.lo.push_back(s.key[i]);
+          s.hi.push_back(s.arg[i]);
+          s.rop.push_back(i);
+          slot = std::max(slot, s.cap[i]);
+          break;
+        case MVBT_OP_INSERT: s.ikeys.push_back(s.key[i]); s.ivals.push_back(s.arg[i]); break;
+        default: s.ekeys.push_back(s.key[i]); break;
+      }
+    }
+    s.slot.push_back(slot);
+    s.pairs += (uint64_t)(s.lo.size() - s.r0.back()) * slot;
+  }
+  s.f0.push_back(s.fkeys.size());
+  s.r0.push_back(s.lo.size());
+  s.i0.push_back(s.ikeys.size());
+  s.e0.push_back(s.ekeys.size());
+  s.p0.push_back(s.pairs);
+  s.pairs += 1024 * stride;  // tail: no query can write past it
+  return s;
+}
+
+struct dstep_t {
+  uint32_t *fk, *fr, *lo, *hi, *cnt, *ik, *iv, *ek;
+  pair_t* pairs;
+};
+
+dstep_t upload(const step_t& s) {
+  dstep_t d;
+  d.fk    = dev_copy(s.fkeys);
+  d.fr    = dev_alloc<uint32_t>(s.fkeys.size());
+  d.lo    = dev_copy(s.lo);
+  d.hi    = dev_copy(s.hi);
+  d.cnt   = dev_alloc<uint32_t>(s.lo.size());
+  d.ik    = dev_copy(s.ikeys);
+  d.iv    = dev_copy(s.ivals);
+  d.ek    = dev_copy(s.ekeys);
+  d.pairs = dev_alloc<pair_t>(s.pairs);
+  check(cudaMemset(d.pairs, 0xFF, s.pairs * sizeof(pair_t)), "memset");
+  return d;
+}
+void release(dstep_t& d) {
+  for (uint32_t* p : {d.fk, d.fr, d.lo, d.hi, d.cnt, d.ik, d.iv, d.ek}) cudaFree(p);
+  cudaFree(d.pairs);
+}
+
+// The reference's plain form, one batch at a time, on the default stream.
+void run_step(vtree_t& tree, const step_t& s, const dstep_t& d) {
+  for (uint32_t b = 0; b < s.nb; ++b) {
+    const uint32_t S  = tree.take_snapshot();
+    const uint64_t nf = s.f0[b + 1] - s.f0[b], nr = s.r0[b + 1] - s.r0[b];
+    const uint64_t ni = s.i0[b + 1] - s.i0[b], ne = s.e0[b + 1] - s.e0[b];
+    if (nf) tree.find(d.fk + s.f0[b], d.fr + s.f0[b], (uint32_t)nf, S, 0, false);
+    if (nr)
+      tree.range_query(d.lo + s.r0[b], d.hi + s.r0[b], d.pairs + s.p0[b], d.cnt + s.r0[b], s.slot[b],
+                       (uint32_t)nr, S, 0, false);
+    if (ni) tree.insert(d.ik + s.i0[b], d.iv + s.i0[b], (uint32_t)ni, 0, true);
+    if (ne) tree.erase(d.ek + s.e0[b], (uint32_t)ne, 0, false);
+  }
+}
+
+void step_checksums(const step_t& s, const dstep_t& d, uint64_t out[3]) {
+  auto fr    = host_copy(d.fr, s.fkeys.size());
+  auto cnt   = host_copy(d.cnt, s.lo.size());
+  auto pairs = host_copy(d.pairs, s.pairs);
+  uint64_t f = 0, c = 0, p = 0;
+  for (uint64_t x = 0; x < fr.size(); ++x) f += find_term(s.fop[x], fr[x]);
+  for (uint32_t b = 0; b < s.nb; ++b) {
+    for (uint64_t x = s.r0[b]; x < s.r0[b + 1]; ++x) {
+      const uint64_t i = s.rop[x];
+      c += count_term(i, cnt[x]);
+      const uint64_t m    = std::min<uint64_t>(cnt[x], s.cap[i]);
+      const pair_t* slot  = pairs.data() + s.p0[b] + (x - s.r0[b]) * s.slot[b];
+      for (uint64_t j = 0; j < m; ++j) p += pair_term(i, j, slot[j].first, slot[j].second);
+    }
+  }
+  out[0] = f;
+  out[1] = c;
+  out[2] = p;
+}
+
+int run_c4(const args_t& a) {
+  mvbt_mix_params p;
+  mvbt_wl_mix_default(&p);
+  const uint64_t stride = a.stride ? a.stride : (0xFFFFFFFDull / 40000000ull);
+  p.stride = (uint32_t)stride;
+  if (a.median > 0) p.batch_median = a.median;
+  if (a.batch_min) p.batch_min = a.batch_min;
+  if (a.batch_max) p.batch_max = a.batch_max;
+
+  std::vector<uint32_t> keys(a.initial), vals(a.initial);
+  mvbt_wl_distinct_keys(a.seed, 0, a.initial, keys.data());
+  mvbt_wl_values(keys.data(), a.initial, 0u, vals.data());
+  void* gen = mvbt_wl_mix_create(&p, a.seed, a.initial);
+
+  // Generate every step first (untimed). Reads allocate nothing; a write adds about one node on
+  // average (a version copy per node and epoch, a split now and then). Refuse workloads whose
+  // generous estimate (4 nodes per write, 4x the initial tree) could reach the pool bound.
+  std::vector<step_t> steps;
+  uint64_t writes = 0;
+  for (uint32_t k = 0; k < a.warmup + a.steps; ++k) {
+    steps.push_back(split(gen, a.batches, stride));
+    writes += steps.back().ikeys.size() + steps.back().ekeys.size();
+  }
+  const uint64_t bound = 4 * (a.initial / 6 + 1) + 4 * writes + 1024;
+  if (bound > kPoolNodes) {
+    std::fprintf(stderr, "ref_driver: workload could exceed the %llu-node pool\n", (unsigned long long)kPoolNodes);
+    return 2;
+  }
+
+  uint32_t *dk = dev_copy(keys), *dv = dev_copy(vals);
+  vtree_t tree;
+  tree.insert(dk, dv, (uint32_t)a.initial, 0, true);
+  check(cudaDeviceSynchronize(), "initial insert");
+  check(cudaGetLastError(), "initial insert");
+  cudaFree(dk);
+  cudaFree(dv);
+
+  cudaEvent_t e0, e1;
+  check(cudaEventCreate(&e0), "event");
+  check(cudaEventCreate(&e1), "event");
+  double timed_ms = 0;
+  uint64_t timed_ops = 0;
+  std::vector<std::vector<uint64_t>> sums;
+  for (uint32_t k = 0; k < a.warmup + a.steps; ++k) {
+    dstep_t d = upload(steps[k]);
+    check(cudaDeviceSynchronize(), "upload");
+    check(cudaEventRecord(e0, 0), "record");
+    run_step(tree, steps[k], d);
+    check(cudaEventRecord(e1, 0), "record");
+    check(cudaEventSynchronize(e1), "step");
+    check(cudaGetLastError(), "step kernels");
+    if (k >= a.warmup) {
+      timed_ms += elapsed_ms(e0, e1);
+      timed_ops += steps[k].num_ops;
+    }
+    if (a.checksums) {
+      uint64_t cs[3];
+      step_checksums(steps[k], d, cs);
+      sums.push_back({cs[0], cs[1], cs[2]});
+    }
+    release(d);
+  }
+
+  // final state: the whole key space as consecutive range queries at a final snapshot
+  uint64_t final_c = 0, final_p = 0;
+  if (a.final_chunks) {
+    const uint32_t C      = a.final_chunks;
+    const uint64_t live   = mvbt_wl_mix_present(gen);
+    const uint64_t span   = (0xFFFFFFFFull - 1 + C - 1) / C;
+    const uint32_t slot   = (uint32_t)std::min<uint64_t>((live / C) * 2 + 1024, 1u << 24);
+    std::vector<uint32_t> lo(C), hi(C);
+    for (uint32_t c = 0; c < C; ++c) {
+      lo[c] = (uint32_t)(1 + c * span);
+      hi[c] = (uint32_t)std::min<uint64_t>(1 + (uint64_t)(c + 1) * span, 0xFFFFFFFFull);
+    }
+    uint32_t *dlo = dev_copy(lo), *dhi = dev_copy(hi), *dcnt = dev_alloc<uint32_t>(C);
+    const uint64_t np = (uint64_t)C * slot + live + 1;  // tail: a chunk returns at most `live` keys
+    pair_t* dp = dev_alloc<pair_t>(np);
+    const uint32_t S = tree.take_snapshot();
+    tree.range_query(dlo, dhi, dp, dcnt, slot, C, S, 0, false);
+    check(cudaDeviceSynchronize(), "final range");
+    check(cudaGetLastError(), "final range");
+    auto cnt   = host_copy(dcnt, C);
+    auto pairs = host_copy(dp, np);
+    for (uint32_t c = 0; c < C; ++c) {
+      final_c += count_term(c, cnt[c]);
+      const uint64_t m = std::min<uint64_t>(cnt[c], slot);
+      for (uint64_t j = 0; j < m; ++j) final_p += pair_term(c, j, pairs[(uint64_t)c * slot + j].first,
+                                                           pairs[(uint64_t)c * slot + j].second);
+    }
+    cudaFree(dlo);
+    cudaFree(dhi);
+    cudaFree(dcnt);
+    cudaFree(dp);
+  }
+  mvbt_wl_mix_destroy(gen);
+
+  std::printf("{\"mode\": \"c4\", \"initial\": %llu, \"batches\": %u, \"steps\": %u, \"warmup\": %u, "
+              "\"seed\": %llu, \"stride\": %llu, \"ops_timed\": %llu, \"ms\": %.4f, \"mops\": %.3f, "
+              "\"final\": [%llu, %llu], \"step_checksums\": [",
+              (unsigned long long)a.initial, a.batches, a.steps, a.warmup, (unsigned long long)a.seed,
+              (unsigned long long)stride, (unsigned long long)timed_ops, timed_ms,
+              timed_ms > 0 ? timed_ops / (timed_ms * 1e3) : 0.0, (unsigned long long)final_c,
+              (unsigned long long)final_p);
+  for (size_t k = 0; k < sums.size(); ++k)
+    std::printf("%s[%llu, %llu, %llu]", k ? ", " : "", (unsigned long long)sums[k][0],
+                (unsigned long long)sums[k][1], (unsigned long long)sums[k][2]);
+  std::printf("]}\n");
+  return 0;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+  args_t a = parse(argc, argv);
+  if (a.mode == "c1") return run_c1(a);
+  if (a.mode == "c4") return run_c4(a);
+  std::fprintf(stderr, "ref_driver: unknown mode %s\n", a.mode.c_str());
+  return 2;
+}
