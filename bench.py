@@ -327,14 +327,16 @@ def run_ours(args, dist: Dist):
     avg_kms = sum(kms) / len(kms)
     peak, peak_kind = measured_hbm_gbs()
     achieved = avg_bytes / (avg_kms * 1e-3) / 1e9
+    mean_ops = sum(steps[s].num_ops for s in range(W, W + K)) / K
+    # DRAM bytes per launch: an ncu capture of one full-size launch of this kernel on this
+    # workload (profiles/k_batched_traffic.json), per op, times the mean ops of the timed launches
     traffic = None
     tf = ROOT / "profiles" / "k_batched_traffic.json"
     if tf.exists():
         try:
-            traffic = json.loads(tf.read_text()).get("dram_bytes_per_launch")
+            traffic = int(json.loads(tf.read_text())["dram_bytes_per_op"] * mean_ops)
         except Exception:
             traffic = None
-    mean_ops = sum(steps[s].num_ops for s in range(W, W + K)) / K
     out = {
         "metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": dist.world,
         "steps": K, "warmup": W, "ms_per_step": round(ms_max / K, 3), "higher_is_better": True,
