@@ -69,7 +69,10 @@ typedef struct mvbt_config {
   uint32_t max_blocks;  /* hard cap on the grid of the bulk kernels (0 = none) */
   uint32_t wait_ms;     /* wall-clock limit of one bounded wait, ms (0 = 2000); a lock queue of
                            every resident tile on one node drains in ~0.1 s */
-  uint32_t reserved[4];
+  uint32_t reclaim;     /* 1 = version copies can be freed (mvbt_reclaim): a retire log and a free
+                           ring of 4 bytes per pool node each, rounded up to powers of two (8 to 16 bytes per node); 0 = keep every
+                           version, as the reference's bump allocator does */
+  uint32_t reserved[3];
 } mvbt_config;
 
 /* Structural report of a host walk over a copy of the node pool (mvbt_validate). */
@@ -91,6 +94,8 @@ typedef struct mvbt_device_view {
   void* control;      /* device control block */
   uint32_t versioned; /* 1 = multiversion tree */
   uint32_t capacity;  /* pool size in nodes */
+  uint32_t reclaim;   /* 1 = the tree was created with config.reclaim (copies go to the retire log) */
+  uint32_t reserved;
 } mvbt_device_view;
 
 void mvbt_config_init(mvbt_config* cfg);
@@ -190,10 +195,25 @@ int mvbt_validate_image_detail(const uint32_t* image, uint64_t nodes, int versio
  * mvbt_validate_image or stored as a dump of the tree. */
 int mvbt_copy_pool(mvbt_tree* tree, void* dst, uint64_t max_nodes, uint64_t* nodes);
 
+#define MVBT_RECLAIM_ALL 0xFFFFFFFFu
+
+/* Frees the version copies that no snapshot id >= min_live_snapshot reads: copies made in write
+ * epochs <= min_live_snapshot. MVBT_RECLAIM_ALL takes the current epoch, after which only the
+ * newest state and snapshots taken later are readable. Freed nodes are reused by later writes.
+ * Stream-ordered: no writer (insert, erase, batch) may run on the tree concurrently with it, and
+ * no reader may use a snapshot below the watermark afterwards (validation at such a snapshot is
+ * undefined too). Needs config.reclaim = 1 (else MVBT_ERR_NOT_SUPPORTED); a no-op on the plain
+ * tree, which makes no copies. Replaces: the epoch-based reclaimer DEBR_device / DEBR_host
+ * (include/memory_reclaimer.hpp:70-410), which frees retired nodes after about two epoch
+ * advances whether or not a snapshot still reads them; here the caller states the oldest live
+ * snapshot. */
+int mvbt_reclaim(mvbt_tree* tree, uint32_t min_live_snapshot, void* stream);
+
 /* Device counters (synchronises the device): out[0] versions copied, [1] node splits, [2] longest
  * locked move-right walk, [3] longest unlocked writer descent, [4] write epoch, [5] error bits,
- * [6..21] errors per raising site, [22] locked approaches restarted unlocked. Writes min(n, 23)
- * values. */
+ * [6..21] errors per raising site, [22] locked approaches restarted unlocked, [23] nodes freed by
+ * mvbt_reclaim, [24] freed nodes waiting for reuse, [25] nodes handed out again, [26] copies the
+ * full retire log could not record (never freed). Writes min(n, 27) values. */
 int mvbt_stats(mvbt_tree* tree, uint64_t* out, uint32_t n);
 
 /* Device view for user kernels calling the cooperative_* device API. */

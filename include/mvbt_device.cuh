@@ -67,6 +67,7 @@
 #include <chrono>
 #include <thread>
 #define MVBT_DEV inline
+#define MVBT_COLD static inline
 struct uint2 {
   uint32_t x, y;
 };
@@ -91,6 +92,12 @@ inline T atomicCAS(T* p, U expected, V desired) {
   return e;
 }
 template <class T, class U>
+inline T atomicMin(T* p, U v) {
+  T cur = __atomic_load_n(p, __ATOMIC_RELAXED);
+  while (cur > (T)v && !__atomic_compare_exchange_n(p, &cur, (T)v, false, __ATOMIC_SEQ_CST, __ATOMIC_RELAXED)) {}
+  return cur;
+}
+template <class T, class U>
 inline T atomicMax(T* p, U v) {
   T cur = __atomic_load_n(p, __ATOMIC_RELAXED);
   while (cur < (T)v && !__atomic_compare_exchange_n(p, &cur, (T)v, false, __ATOMIC_SEQ_CST, __ATOMIC_RELAXED)) {}
@@ -105,6 +112,11 @@ inline thread_local uint32_t sm = 0;  // emulated SM id of the calling lane
 #include <cooperative_groups.h>
 #ifndef MVBT_DEV
 #define MVBT_DEV __device__ __forceinline__
+#endif
+// Rarely taken paths (chunk refills, the retire log). Inlined: an out-of-line call raises the
+// register count of the persistent kernels past the three-blocks-per-SM limit.
+#ifndef MVBT_COLD
+#define MVBT_COLD __device__ __forceinline__
 #endif
 #endif
 
@@ -124,9 +136,17 @@ constexpr uint32_t kNotFound  = 0xFFFFFFFFu;
 constexpr uint32_t kLatest    = 0xFFFFFFFFu;  // read the newest version
 constexpr uint32_t kNone      = 0x0FFFFFFFu;  // "no node" in 28-bit index fields
 constexpr uint32_t kIndexMask = 0x0FFFFFFFu;
-constexpr uint32_t kLockBit   = 0x80000000u;  // in the mod word (node word 27)
-constexpr uint32_t kCountMask = 0x7FFFFFFFu;  // modification count bits of the mod word
-constexpr int kModWord        = 27;
+// Mod word (node word 27): bit 31 lock; bits 0..28 modification count of a live node. A version
+// copy is never locked or changed again, so its mod word records instead that it is retired and
+// the epoch E it was made in (it is read only at snapshots below E); a node that reclamation
+// freed carries kFreeBit until it is reused.
+constexpr uint32_t kLockBit    = 0x80000000u;
+constexpr uint32_t kRetiredBit = 0x40000000u;
+constexpr uint32_t kFreeBit    = 0x20000000u;
+constexpr uint32_t kCountMask  = 0x1FFFFFFFu;  // count (live node) or epoch (retired copy)
+constexpr int kModWord         = 27;
+constexpr uint32_t kRingChunk  = 0x80000000u;  // per-SM chunk base: positions in the free ring
+constexpr uint32_t kReclaimAll = 0xFFFFFFFFu;  // reclaim watermark: the current epoch
 constexpr uint32_t kAnchor    = 0;  // fixed entry node: one entry {0 -> top}, level = top + 1
 constexpr uint32_t kFirstLeaf = 1;  // the initial leaf (holds the tombstone {0, 0})
 constexpr int kMaxLevels      = 16;
@@ -160,6 +180,22 @@ struct control_block {
   unsigned long long stat_restarts;   // locked approaches abandoned for an unlocked re-approach
   uint32_t err_site[16];              // errors per raising site (diagnostics)
   unsigned long long sm_pool[kMaxSmSlots];  // per-SM chunk cursor: (base << 32) | used
+  // Reclamation of version copies (off when reclaim_cap == 0). The retire log holds the index of
+  // every copy made since the last reclaim pass, the free ring the nodes a pass freed; allocation
+  // refills a per-SM chunk from the free ring before the bump pointer.
+  unsigned long long retire_log;   // device address of uint32_t[reclaim_cap]
+  unsigned long long free_ring;    // device address of uint32_t[reclaim_cap]
+  unsigned long long retire_head, retire_tail;  // log positions (monotonic; slot = pos % cap)
+  unsigned long long free_head, free_tail;      // ring positions (monotonic; slot = pos % cap)
+  uint32_t reclaim_cap;     // retire log entries: a power of two >= pool capacity
+  uint32_t rc_pending;      // nodes freed by the running pass
+  uint32_t rc_first_kept;   // first log entry (relative to retire_head) the pass had to keep
+  uint32_t ring_cap;        // free ring slots: a power of two >= capacity + kMaxSmSlots * chunk
+  unsigned long long stat_reclaimed;    // nodes freed by reclaim passes
+  unsigned long long stat_log_dropped;  // copies not logged because the log was full (never freed)
+  unsigned long long stat_reused;       // nodes handed out again from the free ring
+  unsigned long long ring_fail;  // first ring position of a failed chunk pop (~0: none)
+  unsigned long long free_mark;  // ring head at the end of the last pass (for stat_reused)
 };
 
 #if defined(MVBT_HOST_EMULATION)
@@ -188,8 +224,12 @@ MVBT_HD uint32_t initial_tree_word(int t) {
 }
 constexpr int kInitialNodes = 2;
 
+// retire_log / free_ring: device addresses of uint32_t[reclaim_cap] and uint32_t[ring_cap]
+// (powers of two), or 0 with reclaim_cap 0 (reclamation off).
 MVBT_HD void init_control(control_block& c, uint32_t capacity, uint32_t chunk, uint32_t spin_limit,
-                          uint32_t wait_ns) {
+                          uint32_t wait_ns, unsigned long long retire_log = 0,
+                          unsigned long long free_ring = 0, uint32_t reclaim_cap = 0,
+                          uint32_t ring_cap = 0) {
   c.epoch         = 0;
   c.error         = 0;
   c.bump          = kInitialNodes;  // nodes 0 (anchor) and 1 (first leaf)
@@ -206,6 +246,21 @@ MVBT_HD void init_control(control_block& c, uint32_t capacity, uint32_t chunk, u
   for (int i = 0; i < 16; ++i) c.err_site[i] = 0;
   // used == chunk: the first allocation on each SM refills its chunk from the bump pointer
   for (int i = 0; i < kMaxSmSlots; ++i) c.sm_pool[i] = chunk;
+  c.retire_log       = retire_log;
+  c.free_ring        = free_ring;
+  c.retire_head      = 0;
+  c.retire_tail      = 0;
+  c.free_head        = 0;
+  c.free_tail        = 0;
+  c.reclaim_cap      = reclaim_cap;
+  c.rc_pending       = 0;
+  c.rc_first_kept    = 0xFFFFFFFFu;
+  c.ring_cap         = ring_cap;
+  c.stat_reclaimed   = 0;
+  c.stat_log_dropped = 0;
+  c.stat_reused      = 0;
+  c.ring_fail        = ~0ull;
+  c.free_mark        = 0;
 }
 
 // ----------------------------------------------------------------------------------------------
@@ -544,11 +599,45 @@ MVBT_DEV int find_pos(const node_regs<W>& n, uint32_t key, const Tile& t) {
 // ----------------------------------------------------------------------------------------------
 // The tree view: a plain struct passed to kernels by value.
 // ----------------------------------------------------------------------------------------------
+// ---- allocation and retirement slow paths (free functions: no copy of the tree view) ----
+// Node `used` of the chunk that starts at `base`: consecutive nodes of the bump range, or
+// consecutive free-ring positions (kRingChunk set).
+MVBT_DEV uint32_t chunk_node(const control_block* c, uint32_t base, uint32_t used) {
+  if (!(base & kRingChunk)) return base + used;
+  const uint32_t* ring = reinterpret_cast<const uint32_t*>(c->free_ring);
+  return ring[((unsigned long long)(base & ~kRingChunk) + used) & (c->ring_cap - 1u)];
+}
+// Takes C consecutive free-ring positions for a chunk (reclamation on and enough freed nodes):
+// one atomic on the ring head. The ring tail only moves between kernels, so positions below it
+// are written. A pop past the tail fails and records its position; every later pop fails too,
+// and the next reclaim pass moves the head back to the first failed position (those entries were
+// never handed out).
+MVBT_DEV bool take_free_chunk(control_block* c, uint32_t C, uint32_t& base) {
+  const unsigned long long h = atomicAdd(&c->free_head, (unsigned long long)C);
+  if (h + C <= c->free_tail) {
+    base = kRingChunk | (uint32_t)(h & (c->ring_cap - 1u));
+    return true;
+  }
+  atomicMin(&c->ring_fail, h);
+  return false;
+}
+// Records a version copy in the retire log. A copy the full log cannot take is never freed
+// (counted in stat_log_dropped).
+MVBT_COLD void retire_logged(control_block* c, uint32_t copy) {
+  const uint32_t cap           = c->reclaim_cap;
+  const unsigned long long pos = atomicAdd(&c->retire_tail, 1ull);
+  if (pos - ld_relaxed_u64(&c->retire_head) < cap)
+    reinterpret_cast<uint32_t*>(c->retire_log)[pos & (cap - 1u)] = copy;
+  else
+    atomicAdd(&c->stat_log_dropped, 1ull);
+}
+
 struct device_tree {
   uint32_t* pool;       // node words; node i starts at pool + 32 * i
   control_block* ctl;   // device control block
   uint32_t versioned;   // 1 = multiversion tree, 0 = plain B-link tree
   uint32_t capacity;    // pool size in nodes: every index read from memory is checked against it
+  uint32_t reclaim = 0; // 1: version copies go to the retire log (the tree was made with reclaim)
 
   MVBT_DEV uint32_t* node_ptr(uint32_t idx) const { return pool + (size_t)idx * kNodeWords; }
   // An index is dereferenced only after this check; a bad one records kErrCorrupt instead.
@@ -593,7 +682,8 @@ struct device_tree {
   }
   MVBT_DEV uint32_t current_epoch() const { return ld_relaxed_u32(&ctl->epoch); }
 
-  // ---- allocation: per-SM chunks carved from a global bump pointer ----
+  // ---- allocation: per-SM chunks, refilled from the free ring or the global bump pointer ----
+  // Returns a node index, or a free-ring position tagged kRingChunk that alloc() resolves.
   MVBT_DEV uint32_t alloc_one() const {
     control_block* c              = ctl;
     unsigned long long* slot      = &c->sm_pool[sm_id() % kMaxSmSlots];
@@ -606,6 +696,11 @@ struct device_tree {
       uint32_t base = (uint32_t)(old >> 32), used = (uint32_t)old;
       if (used < C) return base + used;
       if (used == C) {  // this thread refills the chunk
+        uint32_t rb = 0;
+        if (reclaim && take_free_chunk(c, C, rb)) {
+          atomicExch(slot, ((unsigned long long)rb << 32) | 1ull);
+          return rb;
+        }
         uint32_t nb = atomicAdd(&c->bump, C);
         if ((unsigned long long)nb + C > c->capacity) {
           atomicOr(&c->error, kErrPoolExhausted);
@@ -633,7 +728,10 @@ struct device_tree {
   MVBT_DEV uint32_t alloc(const Tile& t) const {
     uint32_t idx = kNone;
     if (t.thread_rank() == 0) idx = alloc_one();
-    return t.shfl(idx, 0);
+    idx = t.shfl(idx, 0);
+    // a position in the free ring (a chunk of reclaimed nodes): the node stored there
+    if (idx != kNone && (idx & kRingChunk)) idx = chunk_node(ctl, idx, 0);
+    return idx;
   }
 
   // ---- locks on the mod word ----
@@ -700,7 +798,7 @@ struct device_tree {
       if (copy == kNone) return false;
       node_regs<W> c = n;
       header hc      = h;
-      hc.mod &= kCountMask;  // the copy is never locked
+      hc.mod         = kRetiredBit | (E & kCountMask);  // immutable; read only at snapshots < E
       set_header<W>(c, hc, t);
       store<W>(copy, c, t);
       publish_fence(t);
@@ -709,9 +807,81 @@ struct device_tree {
       set_header<W>(n, h, t);
       store_header<W>(idx, n, t);
       publish_fence(t);
-      if (t.thread_rank() == 0) atomicAdd(&ctl->stat_cow, 1ull);
+      if (t.thread_rank() == 0) retire(copy);
     }
     return true;
+  }
+
+  // ---- reclamation of version copies ----
+  // Records a version copy in the retire log (reclamation on), else counts it.
+  MVBT_DEV void retire(uint32_t copy) const {
+    if (reclaim)
+      retire_logged(ctl, copy);
+    else
+      atomicAdd(&ctl->stat_cow, 1ull);
+  }
+  // One entry of a reclaim pass over the retire log; no writer runs during a pass. A copy made in
+  // epoch E is read only at snapshots below E, so with no live snapshot below the watermark M it
+  // is unreachable once E <= M (compared in a window of 2^28 epochs). Returns 1 if the entry's
+  // copy is now marked free (the caller appends idx to the free ring), 2 if it must be kept, 0 if
+  // the entry was consumed by an earlier pass.
+  MVBT_DEV int reclaim_entry(unsigned long long pos, uint32_t M, uint32_t& idx) const {
+    control_block* c = ctl;
+    uint32_t* slot   = reinterpret_cast<uint32_t*>(c->retire_log) + (pos & (c->reclaim_cap - 1u));
+    idx              = *slot;
+    if (idx >= capacity) return 0;
+    uint32_t* mod    = node_ptr(idx) + kModWord;
+    const uint32_t m = *mod;
+    if (!(m & kRetiredBit)) {
+      *slot = kNone;
+      return 0;
+    }
+    if (((M - m) & kCountMask) > (kCountMask >> 1)) return 2;  // made after the watermark
+    *mod  = kFreeBit;
+    *slot = kNone;
+    return 1;
+  }
+  // End of a reclaim pass, per-SM slot s: the unused rest of its chunk goes back to the free ring
+  // (at positions from ring_tail + *pending on) and the slot is emptied, so no chunk refers to ring
+  // positions a later pass may write. Returns the number of nodes handed back.
+  template <class AddPending>
+  MVBT_DEV uint32_t reclaim_return_chunk(int s, unsigned long long ring_tail, AddPending add_pending) const {
+    control_block* c              = ctl;
+    const uint32_t C              = c->chunk;
+    const unsigned long long v    = c->sm_pool[s];
+    const uint32_t base = (uint32_t)(v >> 32), used = (uint32_t)v;
+    uint32_t n = 0;
+    if (used < C) {
+      n                = C - used;
+      const uint32_t k = add_pending(n);
+      uint32_t* ring   = reinterpret_cast<uint32_t*>(c->free_ring);
+      for (uint32_t u = 0; u < n; ++u) ring[(ring_tail + k + u) & (c->ring_cap - 1u)] = chunk_node(c, base, used + u);
+    }
+    c->sm_pool[s] = C;  // empty: the next allocation on this SM refills
+    return n;
+  }
+  // End of a reclaim pass (one thread, after every entry and every chunk): publishes the
+  // `pushed` ring entries, counts the `freed` copies, moves the log head past consumed entries.
+  // retire_tail stays the count of every copy made. Positions beyond head + capacity were never
+  // written (those copies were dropped); they alias slots this pass marked consumed, so a later
+  // pass passes over them.
+  MVBT_DEV void reclaim_publish(uint32_t pushed, uint32_t freed) const {
+    control_block* c              = ctl;
+    const unsigned long long head = c->retire_head;
+    unsigned long long n          = c->retire_tail - head;
+    if (n > c->reclaim_cap) n = c->reclaim_cap;
+    const uint32_t keep = c->rc_first_kept;
+    c->retire_head      = head + (keep == 0xFFFFFFFFu ? n : keep);
+    unsigned long long fh = c->free_head;
+    if (c->ring_fail < fh) fh = c->ring_fail;  // failed pops handed nothing out
+    c->stat_reused += fh - c->free_mark;
+    c->free_head = fh;
+    c->free_mark = fh;
+    c->ring_fail = ~0ull;
+    c->free_tail += pushed;
+    c->stat_reclaimed += freed;
+    c->rc_pending    = 0;
+    c->rc_first_kept = 0xFFFFFFFFu;
   }
 
   // Moves from node idx to the version visible at ts (snapshot readers only). Sets `copy` when it

@@ -17,6 +17,7 @@ __all__ = [
     "LATEST", "NOT_FOUND", "MVBTError", "lib", "library_path", "gpu_blink_tree",
     "gpu_versioned_btree", "gpu_versioned_blink_tree", "pair_dtype_words", "BatchPlan",
     "BATCH_PERSISTENT", "BATCH_PER_LAUNCH", "BATCH_GRAPH", "NOALLOC_MAX_OPS", "NOALLOC_MAX_BATCHES",
+    "RECLAIM_ALL",
 ]
 
 LATEST = 0xFFFFFFFF
@@ -40,7 +41,7 @@ class mvbt_config(ctypes.Structure):
     _fields_ = [("pool_bytes", _u64), ("device", _i32), ("tile_width", _i32),
                 ("block_size", _i32), ("spin_limit", _u32), ("chunk_nodes", _u32),
                 ("blocks_per_sm", _u32), ("max_blocks", _u32), ("wait_ms", _u32),
-                ("reserved", _u32 * 4)]
+                ("reclaim", _u32), ("reserved", _u32 * 3)]
 
 
 class mvbt_report(ctypes.Structure):
@@ -50,7 +51,8 @@ class mvbt_report(ctypes.Structure):
 
 
 class mvbt_device_view(ctypes.Structure):
-    _fields_ = [("pool", _vp), ("control", _vp), ("versioned", _u32), ("capacity", _u32)]
+    _fields_ = [("pool", _vp), ("control", _vp), ("versioned", _u32), ("capacity", _u32),
+                ("reclaim", _u32), ("reserved", _u32)]
 
 
 def _sig(name, res, *args):
@@ -90,6 +92,7 @@ _sig("mvbt_batch_plan_timing", ctypes.c_int, _vp, ctypes.c_int)
 _sig("mvbt_batch_plan_kernel_times", ctypes.c_int, _vp, ctypes.POINTER(ctypes.c_float), _u32,
      ctypes.POINTER(_u32))
 _sig("mvbt_stats", ctypes.c_int, _vp, ctypes.POINTER(_u64), _u32)
+_sig("mvbt_reclaim", ctypes.c_int, _vp, _u32, _vp)
 _sig("mvbt_batch_run_noalloc", ctypes.c_int, _vp, _u32, _P, _u64, _P, _P, _P, _P, _P, _P, _P, _vp)
 _sig("mvbt_last_error", ctypes.c_char_p)
 _sig("mvbt_status_string", ctypes.c_char_p, ctypes.c_int)
@@ -156,7 +159,8 @@ class _TreeBase:
 
     def __init__(self, pool_bytes: int = 4 << 30, tile_width: int = 8, device: int | None = None,
                  block_size: int = 256, spin_limit: int = 0, chunk_nodes: int = 0,
-                 blocks_per_sm: int = 0, max_blocks: int = 0, wait_ms: int = 0):
+                 blocks_per_sm: int = 0, max_blocks: int = 0, wait_ms: int = 0,
+                 reclaim: bool = False):
         cfg = mvbt_config()
         lib.mvbt_config_init(ctypes.byref(cfg))
         cfg.pool_bytes = int(pool_bytes)
@@ -169,6 +173,7 @@ class _TreeBase:
         cfg.max_blocks = int(max_blocks)
         if wait_ms:
             cfg.wait_ms = int(wait_ms)
+        cfg.reclaim = 1 if reclaim else 0
         h = _vp()
         _check(lib.mvbt_create(self._kind, ctypes.byref(cfg), ctypes.byref(h)), "mvbt_create")
         self._h = h
@@ -284,12 +289,20 @@ class _TreeBase:
 
     def stats(self) -> dict:
         """Device counters: versions copied, splits, longest walks, epoch, error bits per site."""
-        buf = (_u64 * 23)()
-        _check(lib.mvbt_stats(self._h, buf, 23), "stats")
+        buf = (_u64 * 27)()
+        _check(lib.mvbt_stats(self._h, buf, 27), "stats")
         v = list(buf)
         return {"cow": v[0], "splits": v[1], "max_hops": v[2], "max_descent": v[3], "epoch": v[4],
                 "error_bits": v[5], "error_sites": {i: v[6 + i] for i in range(16) if v[6 + i]},
-                "restarts": v[22]}
+                "restarts": v[22], "reclaimed": v[23], "free_nodes": v[24], "reused": v[25],
+                "log_dropped": v[26]}
+
+    def reclaim(self, min_live_snapshot: int = 0xFFFFFFFF, stream=None) -> None:
+        """Frees version copies no snapshot id >= min_live_snapshot reads (RECLAIM_ALL: keep only
+        the newest state and later snapshots). Stream-ordered; no writer may run concurrently.
+        Needs reclaim=True at construction (reference: the DEBR reclaimer,
+        include/memory_reclaimer.hpp:70-410)."""
+        _check(lib.mvbt_reclaim(self._h, int(min_live_snapshot) & 0xFFFFFFFF, _stream(stream)), "reclaim")
 
     def device_view(self) -> mvbt_device_view:
         v = mvbt_device_view()
@@ -342,6 +355,7 @@ class gpu_versioned_btree(_TreeBase):
 
 BATCH_PERSISTENT, BATCH_PER_LAUNCH, BATCH_GRAPH = 0, 1, 2
 NOALLOC_MAX_OPS, NOALLOC_MAX_BATCHES = 1 << 20, 1024  # MVBT_NOALLOC_MAX_OPS / _BATCHES
+RECLAIM_ALL = 0xFFFFFFFF  # MVBT_RECLAIM_ALL
 
 
 class BatchPlan:

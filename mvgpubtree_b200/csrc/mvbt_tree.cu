@@ -30,6 +30,8 @@ struct mvbt_tree {
   control_block* ctl;
   uint32_t* d_words;  // device scratch: [0] snapshot id of the last internal snapshot
   uint32_t* h_word;   // pinned host word
+  uint32_t* retire_log;  // reclamation on: uint32_t[capacity]
+  uint32_t* free_ring;   // reclamation on: uint32_t[capacity + kMaxSmSlots * chunk]
   int num_sms;
   uint32_t spin_limit;
   uint32_t chunk;
@@ -42,6 +44,7 @@ struct mvbt_tree {
     t.ctl       = ctl;
     t.versioned = kind == MVBT_KIND_VERSIONED ? 1u : 0u;
     t.capacity  = (uint32_t)capacity;
+    t.reclaim   = retire_log ? 1u : 0u;
     return t;
   }
 };
@@ -67,9 +70,50 @@ inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s
 // Kernels
 // ----------------------------------------------------------------------------------------------
 __global__ void k_init(uint32_t* pool, control_block* c, uint32_t capacity, uint32_t chunk,
-                       uint32_t spin_limit, uint32_t wait_ns) {
+                       uint32_t spin_limit, uint32_t wait_ns, uint32_t* retire_log, uint32_t* free_ring,
+                       uint32_t log_cap, uint32_t ring_cap) {
   for (int i = threadIdx.x; i < 32 * mvbt::kInitialNodes; i += blockDim.x) pool[i] = mvbt::initial_tree_word(i);
-  if (threadIdx.x == 0) mvbt::init_control(*c, capacity, chunk, spin_limit, wait_ns);
+  if (threadIdx.x == 0)
+    mvbt::init_control(*c, capacity, chunk, spin_limit, wait_ns, (unsigned long long)retire_log,
+                       (unsigned long long)free_ring, log_cap, ring_cap);
+}
+
+// Reclaim pass over the retire log (mvbt_reclaim): frees every version copy made in an epoch <= M
+// (kReclaimAll: the current epoch). Warp-aggregated appends to the free ring.
+__global__ void __launch_bounds__(256) k_reclaim(device_tree T, uint32_t M) {
+  control_block* c              = T.ctl;
+  const unsigned long long head = c->retire_head;
+  unsigned long long n          = c->retire_tail - head;
+  if (n > c->reclaim_cap) n = c->reclaim_cap;
+  if (M == mvbt::kReclaimAll) M = c->epoch;
+  uint32_t* ring                  = reinterpret_cast<uint32_t*>(c->free_ring);
+  const unsigned long long tail   = c->free_tail;
+  const uint32_t lane             = threadIdx.x & 31u;
+  const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+  // b is the same in every lane of a warp, so every lane takes the same number of iterations
+  for (unsigned long long b = (unsigned long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); b < n; b += stride) {
+    const unsigned long long i = b + lane;
+    uint32_t idx               = mvbt::kNone;
+    const int r                = i < n ? T.reclaim_entry(head + i, M, idx) : 0;
+    const uint32_t fm          = __ballot_sync(0xFFFFFFFFu, r == 1);
+    uint32_t first             = 0;
+    if (lane == 0 && fm) first = atomicAdd(&c->rc_pending, (uint32_t)__popc(fm));
+    first = __shfl_sync(0xFFFFFFFFu, first, 0);
+    if (r == 1) ring[(tail + first + __popc(fm & ((1u << lane) - 1u))) & (c->ring_cap - 1u)] = idx;
+    if (r == 2) atomicMin(&c->rc_first_kept, (uint32_t)i);
+  }
+}
+
+// End of a reclaim pass: one block of kMaxSmSlots threads.
+__global__ void k_reclaim_finish(device_tree T) {
+  __shared__ uint32_t freed;
+  control_block* c = T.ctl;
+  if (threadIdx.x == 0) freed = c->rc_pending;
+  __syncthreads();
+  const unsigned long long tail = c->free_tail;
+  T.reclaim_return_chunk((int)threadIdx.x, tail, [&](uint32_t k) { return atomicAdd(&c->rc_pending, k); });
+  __syncthreads();
+  if (threadIdx.x == 0) T.reclaim_publish(c->rc_pending, freed);
 }
 
 __global__ void k_snapshot(control_block* c, uint32_t* out) {
@@ -311,7 +355,20 @@ int mvbt_create(int kind, const mvbt_config* cfg_in, mvbt_tree** out) {
     delete t;
     return fail(MVBT_ERR_OUT_OF_MEMORY, "cudaMalloc of the control block failed");
   }
-  k_init<<<1, 256>>>(t->pool, t->ctl, (uint32_t)capacity, t->chunk, t->spin_limit, t->wait_ms * 1000000u);
+  uint32_t log_cap = 0, ring_cap = 0;
+  if (cfg.reclaim) {  // power-of-two rings: positions map to slots with a mask
+    auto pow2 = [](uint64_t x) { uint64_t p = 1; while (p < x) p <<= 1; return p; };
+    log_cap  = (uint32_t)pow2(capacity);
+    ring_cap = (uint32_t)pow2(capacity + (uint64_t)mvbt::kMaxSmSlots * t->chunk);
+    if (cudaMalloc(&t->retire_log, (uint64_t)log_cap * 4) != cudaSuccess ||
+        cudaMalloc(&t->free_ring, (uint64_t)ring_cap * 4) != cudaSuccess) {
+      cudaGetLastError();
+      mvbt_destroy(t);
+      return fail(MVBT_ERR_OUT_OF_MEMORY, "cudaMalloc of the reclamation rings failed");
+    }
+  }
+  k_init<<<1, 256>>>(t->pool, t->ctl, (uint32_t)capacity, t->chunk, t->spin_limit, t->wait_ms * 1000000u,
+                     t->retire_log, t->free_ring, log_cap, ring_cap);
   e = cudaDeviceSynchronize();
   if (e != cudaSuccess) {
     mvbt_destroy(t);
@@ -328,6 +385,8 @@ int mvbt_destroy(mvbt_tree* t) {
   if (t->pool) cudaFree(t->pool);
   if (t->ctl) cudaFree(t->ctl);
   if (t->d_words) cudaFree(t->d_words);
+  if (t->retire_log) cudaFree(t->retire_log);
+  if (t->free_ring) cudaFree(t->free_ring);
   if (t->h_word) cudaFreeHost(t->h_word);
   delete t;
   return MVBT_OK;
@@ -469,6 +528,19 @@ int mvbt_concurrent_find_erase(mvbt_tree* t, const uint32_t* fkeys, uint32_t* fr
   return check_launch();
 }
 
+int mvbt_reclaim(mvbt_tree* t, uint32_t min_live_snapshot, void* stream) {
+  if (!t) return fail(MVBT_ERR_BAD_ARG, "null tree");
+  if (!t->retire_log)
+    return fail(MVBT_ERR_NOT_SUPPORTED, "reclamation is off: create the tree with mvbt_config.reclaim = 1");
+  MVBT_CUDA_TRY(cudaSetDevice(t->device));
+  cudaStream_t s = as_stream(stream);
+  k_reclaim<<<(unsigned)t->num_sms * 4u, 256, 0, s>>>(t->view(), min_live_snapshot);
+  int st = check_launch();
+  if (st) return st;
+  k_reclaim_finish<<<1, mvbt::kMaxSmSlots, 0, s>>>(t->view());
+  return check_launch();
+}
+
 int mvbt_check_errors(mvbt_tree* t, void* stream, uint32_t* bits) {
   if (!t) return fail(MVBT_ERR_BAD_ARG, "null tree");
   cudaStream_t s = as_stream(stream);
@@ -534,10 +606,17 @@ int mvbt_stats(mvbt_tree* t, uint64_t* out, uint32_t n) {
   MVBT_CUDA_TRY(cudaDeviceSynchronize());
   control_block c;
   MVBT_CUDA_TRY(cudaMemcpy(&c, t->ctl, sizeof(c), cudaMemcpyDeviceToHost));
-  uint64_t v[23] = {c.stat_cow, c.stat_split, c.stat_max_hops, c.stat_max_steps, c.epoch, c.error};
+  const bool rc  = c.reclaim_cap != 0;
+  uint64_t v[27] = {rc ? c.retire_tail : c.stat_cow, c.stat_split, c.stat_max_hops, c.stat_max_steps,
+                    c.epoch, c.error};
   for (int i = 0; i < 16; ++i) v[6 + i] = c.err_site[i];
   v[22] = c.stat_restarts;
-  for (uint32_t i = 0; i < n && i < 23; ++i) out[i] = v[i];
+  v[23] = c.stat_reclaimed;
+  const unsigned long long fh = c.ring_fail < c.free_head ? c.ring_fail : c.free_head;
+  v[24] = rc ? c.free_tail - fh : 0;
+  v[25] = c.stat_reused + (rc ? fh - c.free_mark : 0);
+  v[26] = c.stat_log_dropped;
+  for (uint32_t i = 0; i < n && i < 27; ++i) out[i] = v[i];
   return MVBT_OK;
 }
 
@@ -547,6 +626,8 @@ int mvbt_get_device_view(mvbt_tree* t, mvbt_device_view* out) {
   out->control   = t->ctl;
   out->versioned = t->kind == MVBT_KIND_VERSIONED ? 1u : 0u;
   out->capacity  = (uint32_t)t->capacity;
+  out->reclaim   = t->retire_log ? 1u : 0u;
+  out->reserved  = 0;
   return MVBT_OK;
 }
 

@@ -18,7 +18,8 @@ def lib():
         u32p = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
         vp, u32, u64, i = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int
         sig = {
-            "emu_create": (vp, [i, u32, u32, u32]),
+            "emu_create": (vp, [i, u32, u32, u32, i]),
+            "emu_reclaim": (None, [vp, u32]),
             "emu_destroy": (None, [vp]),
             "emu_errors": (u32, [vp]),
             "emu_bump": (u32, [vp]),
@@ -51,9 +52,9 @@ class EmuTree:
     """A tree held in host memory, operated on by the device code run as host threads."""
 
     def __init__(self, versioned: bool, capacity: int = 1 << 16, tiles: int = 4, W: int = 8,
-                 spin_limit: int = 0, chunk: int = 8):
+                 spin_limit: int = 0, chunk: int = 8, reclaim: bool = False):
         self.L = lib()
-        self.h = self.L.emu_create(int(versioned), capacity, spin_limit, chunk)
+        self.h = self.L.emu_create(int(versioned), capacity, spin_limit, chunk, int(reclaim))
         self.tiles, self.W = tiles, W
 
     def __del__(self):
@@ -66,10 +67,19 @@ class EmuTree:
         return int(self.L.emu_errors(self.h))
 
     def stats(self) -> dict:
-        v = np.zeros(21, np.uint64)
+        v = np.zeros(26, np.uint64)
         self.L.emu_stats(self.h, v)
-        return {"cow": int(v[0]), "splits": int(v[1]), "max_hops": int(v[2]), "max_descent": int(v[3]),
-                "error_sites": {i: int(v[4 + i]) for i in range(16) if v[4 + i]}, "restarts": int(v[20])}
+        return {"cow": int(v[21]), "splits": int(v[1]), "max_hops": int(v[2]), "max_descent": int(v[3]),
+                "error_sites": {i: int(v[4 + i]) for i in range(16) if v[4 + i]}, "restarts": int(v[20]),
+                "reclaimed": int(v[22]), "free_nodes": int(v[23]), "reused": int(v[24]),
+                "log_dropped": int(v[25])}
+
+    def reclaim(self, min_live_snapshot: int = 0xFFFFFFFF):
+        self.L.emu_reclaim(self.h, min_live_snapshot & 0xFFFFFFFF)
+
+    @property
+    def bump(self) -> int:
+        return int(self.L.emu_bump(self.h))
 
     def snapshot(self) -> int:
         return int(self.L.emu_snapshot(self.h))

@@ -52,6 +52,7 @@ struct emu_tile {
 
 struct emu_tree {
   std::vector<uint32_t> pool;
+  std::vector<uint32_t> retire_log, free_ring;  // reclamation on
   mvbt::control_block ctl;
   uint32_t capacity;
   int versioned;
@@ -61,6 +62,7 @@ struct emu_tree {
     t.ctl       = &ctl;
     t.versioned = (uint32_t)versioned;
     t.capacity  = capacity;
+    t.reclaim   = retire_log.empty() ? 0u : 1u;
     return t;
   }
 };
@@ -111,15 +113,54 @@ void run_warps(int warps, int W, const std::function<void(const emu_tile&, const
 
 extern "C" {
 
-void* emu_create(int versioned, uint32_t capacity, uint32_t spin_limit, uint32_t chunk) {
+void* emu_create(int versioned, uint32_t capacity, uint32_t spin_limit, uint32_t chunk, int reclaim) {
   auto* t      = new emu_tree();
   t->capacity  = capacity;
   t->versioned = versioned;
   t->pool.assign((size_t)capacity * 32, 0xA5A5A5A5u);  // garbage, as fresh cudaMalloc memory
   for (int i = 0; i < 32 * mvbt::kInitialNodes; ++i) t->pool[i] = mvbt::initial_tree_word(i);
-  mvbt::init_control(t->ctl, capacity, chunk ? chunk : 8, spin_limit ? spin_limit : (1u << 20),
-                     4000u * 1000u * 1000u);
+  chunk             = chunk ? chunk : 8;
+  uint32_t log_cap  = 0, ring_cap = 0;
+  if (reclaim) {  // the same power-of-two sizes as the library
+    auto pow2 = [](uint64_t x) {
+      uint64_t p = 1;
+      while (p < x) p <<= 1;
+      return (uint32_t)p;
+    };
+    log_cap  = pow2(capacity);
+    ring_cap = pow2((uint64_t)capacity + (uint64_t)mvbt::kMaxSmSlots * chunk);
+    t->retire_log.assign(log_cap, 0xA5A5A5A5u);
+    t->free_ring.assign(ring_cap, 0xA5A5A5A5u);
+  }
+  mvbt::init_control(t->ctl, capacity, chunk, spin_limit ? spin_limit : (1u << 20), 4000u * 1000u * 1000u,
+                     reclaim ? (unsigned long long)t->retire_log.data() : 0ull,
+                     reclaim ? (unsigned long long)t->free_ring.data() : 0ull, log_cap, ring_cap);
   return t;
+}
+
+// A reclaim pass, as mvbt_reclaim runs it (k_reclaim + k_reclaim_finish), single-threaded.
+void emu_reclaim(void* h, uint32_t M) {
+  auto* t = static_cast<emu_tree*>(h);
+  auto v  = t->view();
+  auto& c = t->ctl;
+  if (M == mvbt::kReclaimAll) M = c.epoch;
+  const unsigned long long head = c.retire_head, tail = c.free_tail;
+  const unsigned long long n    = std::min<unsigned long long>(c.retire_tail - head, c.reclaim_cap);
+  uint32_t* ring                = reinterpret_cast<uint32_t*>(c.free_ring);
+  for (unsigned long long i = 0; i < n; ++i) {
+    uint32_t idx = 0;
+    const int r  = v.reclaim_entry(head + i, M, idx);
+    if (r == 1) ring[(tail + c.rc_pending++) & (c.ring_cap - 1u)] = idx;
+    if (r == 2) c.rc_first_kept = std::min<uint32_t>(c.rc_first_kept, (uint32_t)i);
+  }
+  const uint32_t freed = c.rc_pending;
+  for (int s = 0; s < mvbt::kMaxSmSlots; ++s)
+    v.reclaim_return_chunk(s, tail, [&](uint32_t k) {
+      const uint32_t o = c.rc_pending;
+      c.rc_pending += k;
+      return o;
+    });
+  v.reclaim_publish(c.rc_pending, freed);
 }
 
 void emu_destroy(void* h) { delete static_cast<emu_tree*>(h); }
@@ -134,6 +175,12 @@ void emu_stats(void* h, uint64_t* out) {
   out[3] = c.stat_max_steps;
   for (int i = 0; i < 16; ++i) out[4 + i] = c.err_site[i];
   out[20] = c.stat_restarts;
+  out[21] = c.reclaim_cap ? c.retire_tail : c.stat_cow;
+  out[22] = c.stat_reclaimed;
+  const unsigned long long fh = c.ring_fail < c.free_head ? c.ring_fail : c.free_head;
+  out[23] = c.reclaim_cap ? c.free_tail - fh : 0;
+  out[24] = c.stat_reused + (c.reclaim_cap ? fh - c.free_mark : 0);
+  out[25] = c.stat_log_dropped;
 }
 
 uint32_t emu_snapshot(void* h) {

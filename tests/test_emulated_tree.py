@@ -87,6 +87,46 @@ def test_emulated_find_erase_newest_state(w):
     assert np.array_equal(t.find(keys), m.find(keys))
 
 
+@pytest.mark.parametrize("w", [8, 16])
+def test_emulated_reclaim_keeps_live_snapshots_and_reuses_nodes(w):
+    """Rounds of snapshot s, updates and erases, then a reclaim with watermark s: finds at s and
+    at the newest state still match the oracle, freed copies are handed out again, and the
+    allocation high-water mark stops growing."""
+    from emu import EmuTree
+    from mvgpubtree_b200 import workload as wl
+    import oracle
+    seed, n0 = 31, 3000
+    keys = wl.distinct_keys(seed, 0, n0)
+    t = EmuTree(True, capacity=1 << 14, tiles=8, W=w, reclaim=True)
+    m = oracle.MVMap(True)
+    t.insert(keys, wl.values_for(keys, seed))
+    m.insert(keys, wl.values_for(keys, seed))
+    bumps, copies = [], []
+    for r in range(6):
+        s = t.snapshot()
+        assert s == m.take_snapshot()
+        upd = wl.shuffle(seed + r, keys)[:1000]
+        t.insert(upd, wl.values_for(upd, seed + 100 + r))
+        m.insert(upd, wl.values_for(upd, seed + 100 + r))
+        er = wl.shuffle(seed + 50 + r, keys)[:200]
+        t.erase(er)
+        m.erase(er)
+        t.reclaim(s)  # copies made before s are unreadable now; s itself stays readable
+        assert t.errors == 0
+        assert np.array_equal(t.find(keys, s), m.find(keys, s)), f"round {r} at snapshot {s}"
+        assert np.array_equal(t.find(keys), m.find(keys)), f"round {r} newest state"
+        bumps.append(t.bump)
+        copies.append(t.stats()["cow"])
+    st = t.stats()
+    assert st["reclaimed"] > 0 and st["reused"] > 0 and st["log_dropped"] == 0
+    # the last three rounds made many copies but allocated few new nodes: freed ones were reused
+    assert bumps[-1] - bumps[2] < 0.25 * (copies[-1] - copies[2])
+    t.reclaim()  # everything older than the newest state
+    assert np.array_equal(t.find(keys), m.find(keys))
+    rep = t.validate()
+    assert rep["violations"] == 0 and rep["locked_nodes"] == 0
+
+
 def test_emulated_updates_erases_keep_old_snapshots():
     from emu import EmuTree
     from mvgpubtree_b200 import workload as wl
