@@ -14,6 +14,12 @@
  * Keys and values are uint32. Key 0xFFFFFFFF is reserved (an empty slot); 0xFFFFFFFF as a found
  * value is the not-found sentinel. Key 0 starts present with value 0 (the reference's root
  * tombstone). Range queries are half-open [lower, upper).
+ *
+ * Calls that write (insert, erase, the concurrent_* calls, batches, reclaim) must not overlap in
+ * time on different streams: each write call stamps its own epoch, and a versioned tree's
+ * copy-on-write order assumes epochs do not interleave. Readers and writers inside one call are
+ * safe together; so are read-only calls beside anything. As with the reference's host API, the
+ * caller orders the calls.
  */
 #ifndef MVBT_H_
 #define MVBT_H_
@@ -70,8 +76,9 @@ typedef struct mvbt_config {
   uint32_t wait_ms;     /* wall-clock limit of one bounded wait, ms (0 = 2000); a lock queue of
                            every resident tile on one node drains in ~0.1 s */
   uint32_t reclaim;     /* 1 = version copies can be freed (mvbt_reclaim): a retire log and a free
-                           ring of 4 bytes per pool node each, rounded up to powers of two (8 to 16 bytes per node); 0 = keep every
-                           version, as the reference's bump allocator does */
+                           ring of 4 bytes per pool node each, rounded up to powers of two (8 to
+                           16 bytes per node); 0 = keep every version, as the reference's bump
+                           allocator does */
   uint32_t reserved[3];
 } mvbt_config;
 
@@ -283,6 +290,62 @@ int mvbt_batch_run_noalloc(mvbt_tree* tree, uint32_t num_batches, const uint64_t
                            uint64_t num_ops, const uint32_t* type, const uint32_t* key,
                            const uint32_t* arg, const uint64_t* out_off, const uint32_t* range_cap,
                            uint32_t* result, mvbt_pair* range_out, void* stream);
+
+/* ---- Serving: a host request loop with continuous batching ----
+ * mvbt_serve_trace replays a trace of requests (each a batch of mixed ops with an arrival time)
+ * against the tree as a server would: from the session start it admits the requests that have
+ * arrived, in arrival order, as launch slots and node memory allow; every admitted group is one
+ * persistent launch in which each request is its own batch with its own snapshot, so every
+ * query is linearizable at its request's snapshot (reads see all earlier requests' writes, its
+ * own writes follow them). While one launch runs, requests that arrive meanwhile are admitted
+ * into the next one (up to pipeline_depth launches staged or running; copies overlap compute on
+ * a second stream). Between launches a reclaim pass frees the version copies the finished
+ * snapshots read (config.reclaim trees). Results and completion times come back per request.
+ * It has no counterpart in the reference, which has no serving path. */
+typedef struct mvbt_serve_config {
+  uint64_t max_ops_per_launch;      /* ops admitted into one launch (0 = 1 << 21) */
+  uint64_t max_range_pairs;         /* range-output pairs of one launch (0 = 32 * max_ops) */
+  uint32_t max_requests_per_launch; /* requests (batches) in one launch (0 = 1024) */
+  uint32_t pipeline_depth;          /* launches staged or running at once (0 = 2) */
+  uint32_t mode;                    /* MVBT_BATCH_PERSISTENT: continuous batching (default);
+                                       MVBT_BATCH_PER_LAUNCH: one request per launch, the plain
+                                       method, for comparison */
+  uint32_t reclaim_every;           /* launches between reclaim passes; 0 = never (needs
+                                       config.reclaim on the tree otherwise) */
+  uint32_t nodes_per_write;         /* admission: nodes a write may allocate (0 = 3) */
+  uint32_t reserved0;
+  uint64_t reserve_nodes;           /* admission: nodes kept free (0 = 1 << 16) */
+  uint64_t reserved[4];
+} mvbt_serve_config;
+
+typedef struct mvbt_serve_stats {
+  uint64_t requests;      /* requests served */
+  uint64_t ops;           /* ops served */
+  uint64_t launches;      /* launches issued */
+  uint64_t reclaims;      /* reclaim passes issued */
+  uint64_t span_ns;       /* session start to the last completion */
+  uint64_t max_waiting;   /* most requests arrived but not yet admitted at one time */
+  uint64_t memory_waits;  /* admissions deferred until memory was freed */
+  uint64_t max_launch_ops;
+  uint64_t reserved[8];
+} mvbt_serve_stats;
+
+void mvbt_serve_config_init(mvbt_serve_config* cfg);
+
+/* All arrays are HOST arrays; pinned memory (cudaMallocHost) lets the copies run asynchronously.
+ * Request r holds ops [req_off[r], req_off[r + 1]) of type/key/arg/range_cap (as in
+ * mvbt_batch_run) and arrives arrival_ns[r] after the session start (non-decreasing). Range
+ * query i writes at most range_cap[i] pairs at range_out + out_off[i]; the slots of all range
+ * queries must be disjoint and increasing in op order (as mvbt_wl_mix_copy produces them).
+ * Outputs: result[i] per op, the range pairs (a query's slot past its count, and any gap between
+ * slots, is unspecified), done_ns[r] (session clock when the request's results were on the host),
+ * snapshot[r] (the snapshot its reads used; may be null), stats (may be null). Works on the
+ * versioned tree. Synchronises the device. */
+int mvbt_serve_trace(mvbt_tree* tree, const mvbt_serve_config* cfg, uint32_t num_requests,
+                     const uint64_t* req_off, const uint64_t* arrival_ns, const uint32_t* type,
+                     const uint32_t* key, const uint32_t* arg, const uint64_t* out_off,
+                     const uint32_t* range_cap, uint32_t* result, mvbt_pair* range_out,
+                     uint64_t* done_ns, uint32_t* snapshot, mvbt_serve_stats* stats);
 
 /* Tree kind, tile width and device of a handle. */
 int mvbt_get_info(mvbt_tree* tree, int* kind, int* tile_width, int* device);

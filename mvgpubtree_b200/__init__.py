@@ -55,6 +55,18 @@ class mvbt_device_view(ctypes.Structure):
                 ("reclaim", _u32), ("reserved", _u32)]
 
 
+class mvbt_serve_config(ctypes.Structure):
+    _fields_ = [("max_ops_per_launch", _u64), ("max_range_pairs", _u64),
+                ("max_requests_per_launch", _u32), ("pipeline_depth", _u32), ("mode", _u32),
+                ("reclaim_every", _u32), ("nodes_per_write", _u32), ("reserved0", _u32),
+                ("reserve_nodes", _u64), ("reserved", _u64 * 4)]
+
+
+class mvbt_serve_stats(ctypes.Structure):
+    _fields_ = [(n, _u64) for n in ("requests", "ops", "launches", "reclaims", "span_ns", "max_waiting",
+                                     "memory_waits", "max_launch_ops")] + [("reserved", _u64 * 8)]
+
+
 def _sig(name, res, *args):
     f = getattr(lib, name)
     f.restype = res
@@ -93,6 +105,9 @@ _sig("mvbt_batch_plan_kernel_times", ctypes.c_int, _vp, ctypes.POINTER(ctypes.c_
      ctypes.POINTER(_u32))
 _sig("mvbt_stats", ctypes.c_int, _vp, ctypes.POINTER(_u64), _u32)
 _sig("mvbt_reclaim", ctypes.c_int, _vp, _u32, _vp)
+_sig("mvbt_serve_config_init", None, ctypes.POINTER(mvbt_serve_config))
+_sig("mvbt_serve_trace", ctypes.c_int, _vp, ctypes.POINTER(mvbt_serve_config), _u32, _vp, _vp, _vp, _vp,
+     _vp, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.POINTER(mvbt_serve_stats))
 _sig("mvbt_batch_run_noalloc", ctypes.c_int, _vp, _u32, _P, _u64, _P, _P, _P, _P, _P, _P, _P, _vp)
 _sig("mvbt_last_error", ctypes.c_char_p)
 _sig("mvbt_status_string", ctypes.c_char_p, ctypes.c_int)
@@ -346,6 +361,51 @@ class gpu_versioned_btree(_TreeBase):
             _ptr(out_off, 8, "out_off"), _ptr(range_cap, name="range_cap"),
             _ptr(result, name="result"), _ptr(range_out, 8, "range_out"), _stream(stream)),
             "batch_run_noalloc")
+
+    def serve(self, batches, arrival_ns, **config) -> dict:
+        """Serving session over a trace (mvbt_serve_trace): request r is batch r of `batches`
+        (mvgpubtree_b200.workload.Batches, generated in one call so range slots increase) and
+        arrives arrival_ns[r] after the session start. Config keys are the mvbt_serve_config
+        fields (mode, pipeline_depth, max_ops_per_launch, max_requests_per_launch,
+        max_range_pairs, reclaim_every, nodes_per_write, reserve_nodes). Returns numpy arrays
+        result (per op), range_out (pairs, uint32 [n, 2]), done_ns and snapshot (per request),
+        and the stats as a dict. Host buffers are pinned when torch is available."""
+        import numpy as np
+        cfg = mvbt_serve_config()
+        lib.mvbt_serve_config_init(ctypes.byref(cfg))
+        for k, v in config.items():
+            if not hasattr(cfg, k) or k.startswith("reserved"):
+                raise ValueError(f"unknown serving option {k}")
+            setattr(cfg, k, int(v))
+        R = int(batches.num_batches)
+        n = int(batches.num_ops)
+        pairs = max(1, int(batches.range_pairs))
+        try:
+            import torch
+            pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+            empty = lambda count, dt: torch.empty(count, dtype=dt).pin_memory()
+            i32, i64 = torch.int32, torch.int64
+            view = lambda t, dt: t.numpy().view(dt)
+            addr = lambda t: t.data_ptr()
+        except ImportError:  # pageable numpy buffers: the copies run synchronously
+            pin = np.ascontiguousarray
+            empty = lambda count, dt: np.empty(count, dt)
+            i32, i64 = np.int32, np.int64
+            view = lambda t, dt: t.view(dt)
+            addr = lambda t: t.ctypes.data
+        held = [pin(batches.batch_off.view(np.int64)), pin(np.asarray(arrival_ns, np.uint64).view(np.int64)),
+                pin(batches.type.view(np.int32)), pin(batches.key.view(np.int32)),
+                pin(batches.arg.view(np.int32)), pin(batches.out_off.view(np.int64)),
+                pin(batches.range_cap.view(np.int32))]
+        res, rout = empty(max(1, n), i32), empty(pairs * 2, i32)
+        done, snap = empty(R, i64), empty(R, i32)
+        st = mvbt_serve_stats()
+        _check(lib.mvbt_serve_trace(self._h, ctypes.byref(cfg), R, *[addr(h) for h in held], addr(res),
+                                    addr(rout), addr(done), addr(snap), ctypes.byref(st)), "serve_trace")
+        stats = {f: int(getattr(st, f)) for f, _ in mvbt_serve_stats._fields_ if f != "reserved"}
+        return {"result": view(res, np.uint32)[:n].copy(), "range_out": view(rout, np.uint32).reshape(-1, 2).copy(),
+                "done_ns": view(done, np.uint64).copy(), "snapshot": view(snap, np.uint32).copy(),
+                "stats": stats}
 
     def take_snapshot_async(self, d_out, stream=None) -> None:
         """Stream-ordered snapshot; writes the id to the device word d_out."""

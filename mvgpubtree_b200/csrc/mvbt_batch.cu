@@ -334,6 +334,38 @@ int mvbt_batch_plan_destroy(mvbt_batch_plan* p) {
   return MVBT_OK;
 }
 
+// Serving-engine hooks (mvbt_serve.cu). The engine writes a launch's batch offsets straight into
+// the plan's pinned staging and enqueues the persistent run without the stream synchronisation
+// mvbt_batch_run does: it owns one plan per pipeline slot and reuses a plan only after that
+// slot's previous launch has completed.
+uint64_t* mvbt_internal_plan_staging(mvbt_batch_plan* p) { return p->h_batch_off; }
+
+int mvbt_internal_batch_enqueue(mvbt_batch_plan* p, uint32_t num_batches, const uint32_t* type,
+                                const uint32_t* key, const uint32_t* arg, const uint64_t* out_off,
+                                const uint32_t* range_cap, uint32_t* result, mvbt_pair* range_out,
+                                void* stream) {
+  if (!p || num_batches == 0 || num_batches > p->max_batches) return fail(MVBT_ERR_BAD_ARG, "bad batch count");
+  const uint64_t total = p->h_batch_off[num_batches];
+  if (total > p->max_ops) return fail(MVBT_ERR_BAD_ARG, "more ops than the plan holds");
+  launch_ctx c;
+  void* ctl;
+  int st = mvbt_internal_view(p->tree, &c.view, &c.W, &c.block, &c.sms, &c.bps, &c.maxb, &ctl);
+  if (st) return st;
+  c.ctl = static_cast<mvbt::control_block*>(ctl);
+  for (uint32_t b = num_batches + 1; b <= p->max_batches; ++b) p->h_batch_off[b] = total;
+  p->h_params[0] = num_batches;
+  p->h_params[1] = 0;
+  batch_view B;
+  B.type      = type;
+  B.key       = key;
+  B.arg       = arg;
+  B.out_off   = out_off;
+  B.cap       = range_cap;
+  B.result    = result;
+  B.range_out = reinterpret_cast<uint2*>(range_out);
+  return enqueue_persistent(p, c, B, reinterpret_cast<cudaStream_t>(stream));
+}
+
 int mvbt_batch_run(mvbt_batch_plan* p, uint32_t num_batches, const uint64_t* batch_off,
                    const uint32_t* type, const uint32_t* key, const uint32_t* arg,
                    const uint64_t* out_off, const uint32_t* range_cap, uint32_t* result,

@@ -157,3 +157,24 @@ class MixGenerator:
 
     def __del__(self):
         self.close()
+
+
+def serving_trace(seed: int, initial_keys: int, num_requests: int, offered_mops: float, stride: int,
+                  batch_median: float = 256.0, batch_sigma: float = 1.5, batch_min: int = 1,
+                  batch_max: int = 65536):
+    """Requests for a serving session: num_requests mixed batches (the batched mix; sizes
+    lognormal, median 256 ops, clipped [1, 64K]) over the distinct keys [0, initial_keys) of
+    `seed`, and Poisson arrival times (ns from the session start, the first at 0) at an offered
+    load of offered_mops million ops per second (request rate = load / mean request size).
+    Returns (Batches, arrival_ns)."""
+    gen = MixGenerator(seed, initial_keys, stride=stride, batch_median=float(batch_median),
+                       batch_sigma=float(batch_sigma), batch_min=int(batch_min), batch_max=int(batch_max))
+    b = gen.generate(int(num_requests))
+    gen.close()
+    sizes = np.diff(b.batch_off.astype(np.int64))
+    mean = max(1.0, float(sizes.mean()))
+    rate_per_ns = offered_mops * 1e6 / mean / 1e9
+    rng = np.random.default_rng(seed ^ 0x5E12)
+    gaps = rng.exponential(1.0 / rate_per_ns, int(num_requests))
+    gaps[0] = 0.0
+    return b, np.cumsum(gaps).astype(np.uint64)
