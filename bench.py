@@ -14,6 +14,10 @@ e2e      : Mops/s through the public batch API with host buffers: per step the o
            (values, counts and range-output slots) are copied back.
 plain    : the same batches as one snapshot + one launch per batch (the drop-in method).
 roofline : algorithmic bytes of the persistent kernel per launch / its CUDA-event time.
+serving  : continuous batching of Poisson-arriving requests (lognormal sizes, median 256 ops) at
+           offered loads of 10 / 50 / 200 M ops/s for a short window each, on a 40M-key tree with
+           reclamation; p50 / p99 / p999 latency (arrival to results on the host) and achieved
+           throughput, beside the plain mode with one request per launch on an identical tree.
 
 With --impl reference the script times the reference implementation's own CUDA build
 (oracle/_ref/ref_driver, built by oracle/ref_build.py from the reference's unmodified headers) on
@@ -64,6 +68,10 @@ def parse_args():
     ap.add_argument("--cpu-sample-ops", type=int, default=4_000_000,
                     help="ops of the bounded CPU-baseline sample per step")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serve-loads", default="10,50,200",
+                    help="offered loads (M ops/s) of the serving sessions; empty = no serving run")
+    ap.add_argument("--serve-seconds", type=float, default=0.25,
+                    help="arrival window of each serving session")
     return ap.parse_args()
 
 
@@ -367,7 +375,68 @@ def run_ours(args, dist: Dist):
         "clocks": clk,
         "gpu_launches": 5 * K,
     }
+    if args.serve_loads:
+        del plans, pplan, plan, d_ops, d_off, d_cap, d_res, h_res, h_rout, h_in, range_out
+        trees.clear()
+        torch.cuda.empty_cache()
+        out["serving"] = run_serving(args, seed, init, vals, dev)
+        out["serving_p99_us"] = out["serving"]["headline"]["p99_us"]
     return out, (init, vals, steps[W])
+
+
+def latency_summary(arrival_ns, done_ns, ops: int) -> dict:
+    lat = (done_ns.astype(np.int64) - arrival_ns.astype(np.int64)) / 1e3
+    span = float(done_ns.max()) / 1e9
+    return {"achieved_mops": round(ops / span / 1e6, 2), "p50_us": round(float(np.percentile(lat, 50)), 1),
+            "p99_us": round(float(np.percentile(lat, 99)), 1),
+            "p999_us": round(float(np.percentile(lat, 99.9)), 1), "max_us": round(float(lat.max()), 1)}
+
+
+def run_serving(args, seed: int, init, vals, dev) -> dict:
+    """Serving (continuous batching) at each offered load: Poisson arrivals of mixed requests
+    (lognormal sizes, median 256 ops, clipped [1, 64K]) for args.serve_seconds, on a 40M-key tree
+    with reclamation; beside it the plain mode (one request per launch) on an identical tree.
+    Latency = arrival to results on the host; throughput = ops / (start to last completion)."""
+    import torch
+    import mvgpubtree_b200 as mv
+    from mvgpubtree_b200 import workload as wl
+    loads = [float(x) for x in str(args.serve_loads).split(",") if x.strip()]
+    pool = int(args.pool_gb * (1 << 30))
+    trees = {"batched": mv.gpu_versioned_btree(pool_bytes=pool, tile_width=args.tile_width, reclaim=True),
+             "plain": mv.gpu_versioned_btree(pool_bytes=pool, tile_width=args.tile_width)}
+    for t in trees.values():
+        t.insert(dev(init), dev(vals))
+        t.check_errors()
+    gen = wl.serving_generator(seed, args.initial_keys, wl.stride_for(KEYS_40M))  # the trees' key set
+    mean_size = 657.0  # mean of the request-size distribution (lognormal median 256, sigma 1.5)
+    per_load = []
+    for k, load in enumerate(loads):
+        R = max(16, int(load * 1e6 * args.serve_seconds / mean_size))
+        b, arrival = wl.serving_trace(seed + 11 * (k + 1), 0, R, load, 0, generator=gen)
+        res = {"offered_mops": load, "requests": R, "ops": int(b.num_ops)}
+        for name, t in trees.items():
+            o = t.serve(b, arrival, mode=mv.BATCH_PERSISTENT if name == "batched" else mv.BATCH_PER_LAUNCH,
+                        reclaim_every=8 if name == "batched" else 0)
+            t.check_errors()
+            summ = latency_summary(arrival, o["done_ns"], b.num_ops)
+            summ.update({"launches": o["stats"]["launches"], "reclaims": o["stats"]["reclaims"],
+                         "max_waiting": o["stats"]["max_waiting"]})
+            res[name] = summ
+        per_load.append(res)
+    st = trees["batched"].stats()
+    use = trees["batched"].compute_memory_usage()
+    head = next((r for r in per_load if r["offered_mops"] == 50.0), per_load[-1])
+    gen.close()
+    return {"mode": "continuous batching: the requests that arrived while the previous launch ran "
+                    "form the next launch, one snapshot per admitted batch (reads at it, writes after), "
+                    "reclaim every 8 launches",
+            "request_size": "lognormal median 256 ops, sigma 1.5, clipped [1, 65536]",
+            "arrivals": "Poisson", "seconds_per_load": args.serve_seconds, "pool_gb": args.pool_gb,
+            "per_load": per_load,
+            "headline": {"offered_mops": head["offered_mops"], **{k: head["batched"][k] for k in
+                         ("achieved_mops", "p50_us", "p99_us", "p999_us")}},
+            "reclaimed_nodes": st["reclaimed"], "reused_nodes": st["reused"],
+            "nodes_high_water": use["nodes_allocated"]}
 
 
 # ------------------------------------------------------------------------------------------------

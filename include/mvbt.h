@@ -294,14 +294,22 @@ int mvbt_batch_run_noalloc(mvbt_tree* tree, uint32_t num_batches, const uint64_t
 /* ---- Serving: a host request loop with continuous batching ----
  * mvbt_serve_trace replays a trace of requests (each a batch of mixed ops with an arrival time)
  * against the tree as a server would: from the session start it admits the requests that have
- * arrived, in arrival order, as launch slots and node memory allow; every admitted group is one
- * persistent launch in which each request is its own batch with its own snapshot, so every
- * query is linearizable at its request's snapshot (reads see all earlier requests' writes, its
- * own writes follow them). While one launch runs, requests that arrive meanwhile are admitted
- * into the next one (up to pipeline_depth launches staged or running; copies overlap compute on
- * a second stream). Between launches a reclaim pass frees the version copies the finished
- * snapshots read (config.reclaim trees). Results and completion times come back per request.
- * It has no counterpart in the reference, which has no serving path. */
+ * arrived, in arrival order, as launch slots and node memory allow, and runs every admitted
+ * group as one persistent launch. With MVBT_SERVE_SNAPSHOT_PER_BATCH (the default) the group is
+ * one batch with one snapshot: every read of the group sees the state after all earlier groups,
+ * every write lands after them, so each query is linearizable at its group's snapshot (requests
+ * admitted together were concurrent). With MVBT_SERVE_SNAPSHOT_PER_REQUEST each request is its
+ * own batch with its own snapshot: reads also see the writes of earlier requests of the group
+ * (sequential order; slower, as each batch's reads wait for the previous batch's writes).
+ * While one launch runs, requests that arrive meanwhile are admitted into the next one (up to
+ * pipeline_depth launches staged or running; copies overlap compute on two more streams).
+ * Between launches a reclaim pass frees the version copies the finished snapshots read
+ * (config.reclaim trees). Results and completion times come back per request. Requests of one
+ * group must not write the same key (a trace from mvbt_wl_mix_* with erase_lag above
+ * max_requests_per_launch guarantees it). It has no counterpart in the reference, which has no
+ * serving path. */
+#define MVBT_SERVE_SNAPSHOT_PER_BATCH 0u
+#define MVBT_SERVE_SNAPSHOT_PER_REQUEST 1u
 typedef struct mvbt_serve_config {
   uint64_t max_ops_per_launch;      /* ops admitted into one launch (0 = 1 << 21) */
   uint64_t max_range_pairs;         /* range-output pairs of one launch (0 = 32 * max_ops) */
@@ -313,7 +321,7 @@ typedef struct mvbt_serve_config {
   uint32_t reclaim_every;           /* launches between reclaim passes; 0 = never (needs
                                        config.reclaim on the tree otherwise) */
   uint32_t nodes_per_write;         /* admission: nodes a write may allocate (0 = 3) */
-  uint32_t reserved0;
+  uint32_t snapshots;               /* MVBT_SERVE_SNAPSHOT_PER_BATCH (0) or _PER_REQUEST */
   uint64_t reserve_nodes;           /* admission: nodes kept free (0 = 1 << 16) */
   uint64_t reserved[4];
 } mvbt_serve_config;
@@ -339,8 +347,8 @@ void mvbt_serve_config_init(mvbt_serve_config* cfg);
  * queries must be disjoint and increasing in op order (as mvbt_wl_mix_copy produces them).
  * Outputs: result[i] per op, the range pairs (a query's slot past its count, and any gap between
  * slots, is unspecified), done_ns[r] (session clock when the request's results were on the host),
- * snapshot[r] (the snapshot its reads used; may be null), stats (may be null). Works on the
- * versioned tree. Synchronises the device. */
+ * snapshot[r] (the snapshot its reads used: requests with the same one formed one group; may be
+ * null), stats (may be null). Works on the versioned tree. Synchronises the device. */
 int mvbt_serve_trace(mvbt_tree* tree, const mvbt_serve_config* cfg, uint32_t num_requests,
                      const uint64_t* req_off, const uint64_t* arrival_ns, const uint32_t* type,
                      const uint32_t* key, const uint32_t* arg, const uint64_t* out_off,

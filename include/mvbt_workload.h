@@ -54,7 +54,11 @@ typedef struct mvbt_mix_params {
   uint32_t stride;      /* key distance per unit of L: upper = lower + L * stride */
   uint32_t value_salt;  /* values are fmix32(key ^ salt) */
   uint32_t fixed_batch; /* nonzero: every batch has exactly this many ops */
-  uint32_t reserved[3];
+  uint32_t erase_lag;   /* batches before an inserted key can be erased or picked as a find hit
+                           (0 = from the next batch on); a serving trace whose requests may share
+                           one snapshot uses more than a launch's requests, so no request erases
+                           a key another request of its launch inserts */
+  uint32_t reserved[2];
 } mvbt_mix_params;
 
 void mvbt_wl_mix_default(mvbt_mix_params* p);

@@ -17,7 +17,7 @@ __all__ = [
     "LATEST", "NOT_FOUND", "MVBTError", "lib", "library_path", "gpu_blink_tree",
     "gpu_versioned_btree", "gpu_versioned_blink_tree", "pair_dtype_words", "BatchPlan",
     "BATCH_PERSISTENT", "BATCH_PER_LAUNCH", "BATCH_GRAPH", "NOALLOC_MAX_OPS", "NOALLOC_MAX_BATCHES",
-    "RECLAIM_ALL",
+    "RECLAIM_ALL", "SERVE_SNAPSHOT_PER_BATCH", "SERVE_SNAPSHOT_PER_REQUEST",
 ]
 
 LATEST = 0xFFFFFFFF
@@ -58,7 +58,7 @@ class mvbt_device_view(ctypes.Structure):
 class mvbt_serve_config(ctypes.Structure):
     _fields_ = [("max_ops_per_launch", _u64), ("max_range_pairs", _u64),
                 ("max_requests_per_launch", _u32), ("pipeline_depth", _u32), ("mode", _u32),
-                ("reclaim_every", _u32), ("nodes_per_write", _u32), ("reserved0", _u32),
+                ("reclaim_every", _u32), ("nodes_per_write", _u32), ("snapshots", _u32),
                 ("reserve_nodes", _u64), ("reserved", _u64 * 4)]
 
 
@@ -366,8 +366,9 @@ class gpu_versioned_btree(_TreeBase):
         """Serving session over a trace (mvbt_serve_trace): request r is batch r of `batches`
         (mvgpubtree_b200.workload.Batches, generated in one call so range slots increase) and
         arrives arrival_ns[r] after the session start. Config keys are the mvbt_serve_config
-        fields (mode, pipeline_depth, max_ops_per_launch, max_requests_per_launch,
-        max_range_pairs, reclaim_every, nodes_per_write, reserve_nodes). Returns numpy arrays
+        fields (mode, snapshots: SERVE_SNAPSHOT_PER_BATCH or _PER_REQUEST, pipeline_depth,
+        max_ops_per_launch, max_requests_per_launch, max_range_pairs, reclaim_every,
+        nodes_per_write, reserve_nodes). Returns numpy arrays
         result (per op), range_out (pairs, uint32 [n, 2]), done_ns and snapshot (per request),
         and the stats as a dict. Host buffers are pinned when torch is available."""
         import numpy as np
@@ -416,6 +417,7 @@ class gpu_versioned_btree(_TreeBase):
 BATCH_PERSISTENT, BATCH_PER_LAUNCH, BATCH_GRAPH = 0, 1, 2
 NOALLOC_MAX_OPS, NOALLOC_MAX_BATCHES = 1 << 20, 1024  # MVBT_NOALLOC_MAX_OPS / _BATCHES
 RECLAIM_ALL = 0xFFFFFFFF  # MVBT_RECLAIM_ALL
+SERVE_SNAPSHOT_PER_BATCH, SERVE_SNAPSHOT_PER_REQUEST = 0, 1  # MVBT_SERVE_SNAPSHOT_*
 
 
 class BatchPlan:

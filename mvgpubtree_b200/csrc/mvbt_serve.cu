@@ -132,6 +132,7 @@ int mvbt_serve_trace(mvbt_tree* tree, const mvbt_serve_config* cfg_in, uint32_t 
     if (!cfg.nodes_per_write) cfg.nodes_per_write = 3;
     if (!cfg.reserve_nodes) cfg.reserve_nodes = 1ull << 16;
   }
+  if (cfg.snapshots > MVBT_SERVE_SNAPSHOT_PER_REQUEST) return fail(MVBT_ERR_BAD_ARG, "unknown snapshots mode");
   if (cfg.mode != MVBT_BATCH_PERSISTENT && cfg.mode != MVBT_BATCH_PER_LAUNCH)
     return fail(MVBT_ERR_BAD_ARG, "serving mode must be MVBT_BATCH_PERSISTENT or MVBT_BATCH_PER_LAUNCH");
   if (cfg.pipeline_depth > 8) return fail(MVBT_ERR_BAD_ARG, "pipeline_depth is at most 8");
@@ -159,6 +160,8 @@ int mvbt_serve_trace(mvbt_tree* tree, const mvbt_serve_config* cfg_in, uint32_t 
   if (cfg.reclaim_every && !view.reclaim)
     return fail(MVBT_ERR_NOT_SUPPORTED, "reclaim_every needs a tree created with config.reclaim = 1");
   const uint32_t max_req = cfg.mode == MVBT_BATCH_PER_LAUNCH ? 1u : cfg.max_requests_per_launch;
+  // batches per launch: one per request, or the whole admitted group as one batch
+  const bool per_request = cfg.snapshots == MVBT_SERVE_SNAPSHOT_PER_REQUEST;
 
   // per request: write count and range-output region [rp0, rp1) (slots increase in op order)
   std::vector<uint64_t> rp0(R), rp1(R), writes(R);
@@ -196,7 +199,7 @@ int mvbt_serve_trace(mvbt_tree* tree, const mvbt_serve_config* cfg_in, uint32_t 
   S.slots.resize(cfg.pipeline_depth);
   const uint64_t mo = cfg.max_ops_per_launch, mp = cfg.max_range_pairs;
   for (auto& s : S.slots) {
-    st = mvbt_batch_plan_create(tree, mo, max_req, &s.plan);
+    st = mvbt_batch_plan_create(tree, mo, per_request ? max_req : 1u, &s.plan);
     if (st) return st;
     SERVE_TRY(cudaMalloc(&s.type, mo * 4));
     SERVE_TRY(cudaMalloc(&s.key, mo * 4));
@@ -257,8 +260,12 @@ int mvbt_serve_trace(mvbt_tree* tree, const mvbt_serve_config* cfg_in, uint32_t 
     if (n) {
       if (cfg.mode == MVBT_BATCH_PERSISTENT) {
         uint64_t* stage = mvbt_internal_plan_staging(s.plan);
-        for (uint32_t b = 0; b <= nb; ++b) stage[b] = req_off[r0 + b] - o0;
-        int es = mvbt_internal_batch_enqueue(s.plan, nb, s.type, s.key, s.arg, s.off, s.cap, s.result, shifted, S.cs);
+        const uint32_t lb = per_request ? nb : 1u;
+        if (per_request)
+          for (uint32_t b = 0; b <= nb; ++b) stage[b] = req_off[r0 + b] - o0;
+        else
+          stage[0] = 0, stage[1] = n;
+        int es = mvbt_internal_batch_enqueue(s.plan, lb, s.type, s.key, s.arg, s.off, s.cap, s.result, shifted, S.cs);
         if (es) return es;
       } else {
         const uint64_t one[2] = {0, n};
@@ -277,9 +284,10 @@ int mvbt_serve_trace(mvbt_tree* tree, const mvbt_serve_config* cfg_in, uint32_t 
     SERVE_TRY(cudaEventRecord(s.done, S.ys));
     // an empty request still takes its snapshot in the persistent path; the per-launch path
     // takes one per launch
+    const bool own = per_request || cfg.mode == MVBT_BATCH_PER_LAUNCH;  // a snapshot per request
     for (uint32_t b = 0; b < nb; ++b)
-      if (snapshot) snapshot[r0 + b] = epoch + b;
-    epoch += n ? nb : 0;
+      if (snapshot) snapshot[r0 + b] = own ? epoch + b : epoch;
+    epoch += n ? (own ? nb : 1u) : 0u;
     s.r0 = r0;
     s.r1 = r1;
     s.reserve = reserve;

@@ -5,6 +5,7 @@
 // distinct uniform draws from [1, 2^32 - 3] instead of a dense iota, values are fmix32(key ^ salt).
 #include <algorithm>
 #include <cmath>
+#include <deque>
 #include <cstdint>
 #include <cstring>
 #include <thread>
@@ -73,6 +74,10 @@ struct MixGen {
   Feistel f;
   uint64_t rng;
   std::vector<uint32_t> present;
+  // keys inserted in the last erase_lag batches (batch number, key): present in the tree, but
+  // neither erased nor picked as find hits until they join `present`
+  std::deque<std::pair<uint64_t, uint32_t>> young;
+  uint64_t batch_no = 0;
   uint64_t next_insert;
   uint64_t next_miss = MVBT_MISS_INDEX_BASE;
   // last generated batches
@@ -112,7 +117,11 @@ struct MixGen {
     out_off.clear();
     uint64_t pairs = 0;
     const double c1 = p.p_erase, c2 = c1 + p.p_insert, c3 = c2 + p.p_find;
-    for (uint32_t b = 0; b < nb; ++b) {
+    for (uint32_t b = 0; b < nb; ++b, ++batch_no) {
+      while (!young.empty() && young.front().first + p.erase_lag <= batch_no) {
+        present.push_back(young.front().second);
+        young.pop_front();
+      }
       uint64_t size;
       if (p.fixed_batch) {
         size = p.fixed_batch;
@@ -133,7 +142,7 @@ struct MixGen {
         type[base + i] = u < c1 ? MVBT_OP_ERASE : (u < c2 ? MVBT_OP_INSERT : (u < c3 ? MVBT_OP_FIND : MVBT_OP_RANGE));
       }
       const uint64_t n_present = present.size();
-      const double density     = (double)(n_present + 1) / 4294967296.0;
+      const double density     = (double)(n_present + young.size() + 1) / 4294967296.0;
       // pass 1: reads (they see the state at the batch snapshot: the present set as it is now)
       for (uint64_t i = 0; i < size; ++i) {
         const uint64_t o = base + i;
@@ -184,7 +193,10 @@ struct MixGen {
         arg[o]     = fmix32(k ^ p.value_salt);
         cap[o]     = 0;
         out_off[o] = 0;
-        present.push_back(k);
+        if (p.erase_lag)
+          young.emplace_back(batch_no, k);
+        else
+          present.push_back(k);
       }
       batch_off.push_back(type.size());
     }
@@ -277,6 +289,9 @@ void mvbt_wl_mix_copy(void* h, uint64_t* batch_off, uint32_t* type, uint32_t* ke
   if (range_cap) std::memcpy(range_cap, g->cap.data(), n * 4);
 }
 
-uint64_t mvbt_wl_mix_present(void* h) { return static_cast<MixGen*>(h)->present.size(); }
+uint64_t mvbt_wl_mix_present(void* h) {
+  auto* g = static_cast<MixGen*>(h);
+  return g->present.size() + g->young.size();
+}
 
 }  // extern "C"

@@ -29,7 +29,7 @@ class mvbt_mix_params(ctypes.Structure):
                 ("batch_sigma", ctypes.c_double), ("batch_min", _u32), ("batch_max", _u32),
                 ("range_mean", ctypes.c_double), ("range_min", _u32), ("range_max", _u32),
                 ("stride", _u32), ("value_salt", _u32), ("fixed_batch", _u32),
-                ("reserved", _u32 * 3)]
+                ("erase_lag", _u32), ("reserved", _u32 * 2)]
 
 
 def _sig(name, res, *args):
@@ -159,18 +159,32 @@ class MixGenerator:
         self.close()
 
 
+def serving_generator(seed: int, initial_keys: int, stride: int, batch_median: float = 256.0,
+                      batch_sigma: float = 1.5, batch_min: int = 1, batch_max: int = 65536,
+                      erase_lag: int = 4096):
+    """Request generator of the serving workload (the batched mix; request sizes lognormal,
+    median 256 ops, clipped [1, 64K]) over the distinct keys [0, initial_keys) of `seed`. A key a
+    request inserts can be erased (or picked as a find hit) only erase_lag requests later, more
+    than one launch admits, so requests that share a snapshot never write the same key."""
+    return MixGenerator(seed, initial_keys, stride=stride, batch_median=float(batch_median),
+                        batch_sigma=float(batch_sigma), batch_min=int(batch_min), batch_max=int(batch_max),
+                        erase_lag=int(erase_lag))
+
+
 def serving_trace(seed: int, initial_keys: int, num_requests: int, offered_mops: float, stride: int,
                   batch_median: float = 256.0, batch_sigma: float = 1.5, batch_min: int = 1,
-                  batch_max: int = 65536):
-    """Requests for a serving session: num_requests mixed batches (the batched mix; sizes
-    lognormal, median 256 ops, clipped [1, 64K]) over the distinct keys [0, initial_keys) of
-    `seed`, and Poisson arrival times (ns from the session start, the first at 0) at an offered
-    load of offered_mops million ops per second (request rate = load / mean request size).
-    Returns (Batches, arrival_ns)."""
-    gen = MixGenerator(seed, initial_keys, stride=stride, batch_median=float(batch_median),
-                       batch_sigma=float(batch_sigma), batch_min=int(batch_min), batch_max=int(batch_max))
+                  batch_max: int = 65536, generator: "MixGenerator | None" = None,
+                  erase_lag: int = 4096):
+    """Requests for a serving session: num_requests mixed batches from `generator` (default: a new
+    serving_generator over the distinct keys [0, initial_keys) of `seed`; pass one to continue a
+    key set across sessions), and Poisson arrival times (ns from the session start, the first at
+    0) at an offered load of offered_mops million ops per second (request rate = load / mean
+    request size). Returns (Batches, arrival_ns)."""
+    gen = generator or serving_generator(seed, initial_keys, stride, batch_median, batch_sigma,
+                                         batch_min, batch_max, erase_lag)
     b = gen.generate(int(num_requests))
-    gen.close()
+    if generator is None:
+        gen.close()
     sizes = np.diff(b.batch_off.astype(np.int64))
     mean = max(1.0, float(sizes.mean()))
     rate_per_ns = offered_mops * 1e6 / mean / 1e9

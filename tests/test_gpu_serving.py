@@ -1,10 +1,12 @@
 """GPU tier: the serving loop (mvbt_serve_trace), continuous batching over the persistent path.
 
-A trace of mixed requests with Poisson arrivals is served with several requests per launch and
-reclamation between launches. Every request's results must be
-  * the oracle's for that request applied after all earlier requests (bit-exact), and
-  * the same as the request run alone, in the same order, on an identical tree (one batch per
-    launch), and as in the plain mode with one request per launch.
+A trace of mixed requests with Poisson arrivals is served with several requests per launch.
+  * One snapshot per admitted batch (the default): requests admitted together share a snapshot.
+    Their results must equal the oracle's with the same groups applied as batches, and each
+    group's reads run alone afterwards at its snapshot must return the same results.
+  * One snapshot per request: every request's results must equal the oracle's for that request
+    applied after all earlier requests, the request run alone in the same order on an identical
+    tree, and the plain mode with one request per launch.
 """
 import numpy as np
 import pytest
@@ -50,15 +52,70 @@ def make_tree(torch, mv, wl, initial, seed, w, reclaim):
 
 
 @pytest.mark.parametrize("w", [8, 16])
-def test_served_requests_match_oracle_and_alone(torch, w):
+def test_served_groups_match_oracle_and_alone_at_their_snapshot(torch, w):
+    from mvgpubtree_b200 import workload as wl
+    import mvgpubtree_b200 as mv
+    import oracle
+    initial, seed, R = 100_000, 91, 1500
+    b, arrival = wl.serving_trace(seed, initial, R, offered_mops=40.0, stride=wl.stride_for(initial),
+                                  batch_max=8192, erase_lag=128)
+    t, init = make_tree(torch, mv, wl, initial, seed, w, reclaim=False)  # keep every snapshot
+    out = t.serve(b, arrival, max_requests_per_launch=64)
+    assert t.check_errors() == 0
+    st = out["stats"]
+    assert st["requests"] == R and st["launches"] < R, st
+    snaps = out["snapshot"].astype(np.int64)
+    steps = np.diff(snaps)
+    assert np.all((steps == 0) | (steps == 1))  # groups in order, one snapshot each
+    starts = np.concatenate([[0], np.nonzero(steps)[0] + 1, [R]])
+    group_off = b.batch_off[starts].astype(np.uint64)
+    served = range_views(b, out["result"], out["range_out"])
+    find = b.type == 0
+    # the oracle with the same groups applied as batches
+    m = oracle.MVMap(True)
+    m.insert(init, wl.values_for(init, 0))
+    g = wl.Batches(group_off, b.type, b.key, b.arg, b.out_off, b.range_cap, b.range_pairs)
+    er, eo = m.run_batches(g)
+    assert np.array_equal(out["result"][find], er[find])
+    assert served == range_views(b, er, eo.reshape(-1, 2))
+    # each group's reads alone, afterwards, at the group's snapshot
+    for k in range(len(starts) - 1):
+        lo, hi = int(group_off[k]), int(group_off[k + 1])
+        S = int(snaps[starts[k]])
+        ty = b.type[lo:hi]
+        fk = b.key[lo:hi][ty == 0]
+        if fk.size:
+            o = torch.empty(fk.size, dtype=torch.int32, device="cuda")
+            t.find(dev(torch, fk), o, timestamp=S)
+            assert np.array_equal(host(o), out["result"][lo:hi][ty == 0]), f"group {k} finds"
+        rq = np.nonzero(ty == 3)[0]
+        if rq.size:
+            cap = int(b.range_cap[lo:hi][rq].max())
+            pr = torch.full((rq.size * cap * 2,), -1, dtype=torch.int32, device="cuda")
+            cn = torch.empty(rq.size, dtype=torch.int32, device="cuda")
+            t.range_query(dev(torch, b.key[lo:hi][rq]), dev(torch, b.arg[lo:hi][rq]), pr, cn, cap,
+                          rq.size, S)
+            alone = host(pr).reshape(rq.size, cap, 2)
+            counts = host(cn)
+            for j, i in enumerate(rq):
+                op = lo + int(i)
+                c, m_ = int(counts[j]), min(int(counts[j]), int(b.range_cap[op]))
+                o_ = int(b.out_off[op])
+                assert c == int(out["result"][op]), f"group {k} range count"
+                assert alone[j, :m_].tobytes() == out["range_out"][o_:o_ + m_].tobytes(), f"group {k} pairs"
+
+
+@pytest.mark.parametrize("w", [8, 16])
+def test_per_request_snapshots_match_oracle_and_alone(torch, w):
     from mvgpubtree_b200 import workload as wl
     import mvgpubtree_b200 as mv
     import oracle
     initial, seed, R = 100_000, 77, 1200
     b, arrival = wl.serving_trace(seed, initial, R, offered_mops=20.0, stride=wl.stride_for(initial),
-                                  batch_max=8192)
+                                  batch_max=8192, erase_lag=0)
     t, init = make_tree(torch, mv, wl, initial, seed, w, reclaim=True)
-    out = t.serve(b, arrival, reclaim_every=4, max_requests_per_launch=64)
+    out = t.serve(b, arrival, reclaim_every=4, max_requests_per_launch=64,
+                  snapshots=mv.SERVE_SNAPSHOT_PER_REQUEST)
     assert t.check_errors() == 0
     st = out["stats"]
     assert st["requests"] == R and st["ops"] == b.num_ops
@@ -103,7 +160,7 @@ def test_served_requests_match_oracle_and_alone(torch, w):
     assert served == range_views(b, res, rout)
     # the plain mode, one request per launch, on an identical tree
     p, _ = make_tree(torch, mv, wl, initial, seed, w, reclaim=False)
-    plain = p.serve(b, arrival, mode=mv.BATCH_PER_LAUNCH)
+    plain = p.serve(b, arrival, mode=mv.BATCH_PER_LAUNCH, snapshots=mv.SERVE_SNAPSHOT_PER_REQUEST)
     assert plain["stats"]["launches"] == np.count_nonzero(np.diff(b.batch_off.astype(np.int64)))
     bad = np.nonzero(find & (plain["result"] != out["result"]))[0]
     assert bad.size == 0, (
