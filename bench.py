@@ -68,6 +68,8 @@ def parse_args():
     ap.add_argument("--cpu-sample-ops", type=int, default=4_000_000,
                     help="ops of the bounded CPU-baseline sample per step")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep --tile-width / --blocks-per-sm instead of tuning the launch shape")
     ap.add_argument("--serve-loads", default="10,50,200",
                     help="offered loads (M ops/s) of the serving sessions; empty = no serving run")
     ap.add_argument("--serve-seconds", type=float, default=0.25,
@@ -238,6 +240,12 @@ def run_ours(args, dist: Dist):
         trees[name] = t
     torch.cuda.synchronize()
     plans = {k: t.batch_plan(max_ops, args.batches) for k, t in trees.items()}
+    # launch shape of the persistent path: autotuned on clones of the tree with the first two
+    # steps of the workload (the timed steps come later and are not part of the sample)
+    tune = None
+    if not args.no_autotune:
+        from mvgpubtree_b200.autotune import autotune_batches
+        tune = autotune_batches(trees["batched"], steps[:2], plan=plans["batched"])
     range_out = torch.empty(max(1, max_pairs) * 2, dtype=torch.int32, device="cuda")
     stream = torch.cuda.current_stream()
 
@@ -356,7 +364,9 @@ def run_ours(args, dist: Dist):
             "initial_keys": args.initial_keys, "batches_per_step": args.batches,
             "batch_size": "lognormal median 16384, sigma 1.5, clipped [1024, 4194304]",
             "mean_ops_per_step": int(mean_ops), "mode": "persistent launch, device work queue",
-            "tile_width": args.tile_width, "blocks_per_sm": args.blocks_per_sm,
+            "tile_width": tune["tile_width"] if tune else args.tile_width,
+            "blocks_per_sm": tune["blocks_per_sm"] if tune else args.blocks_per_sm,
+            "autotune": tune,
             "parallelism": f"replicas x{dist.world}",
             "l2": "inputs larger than L2 (tree of %d nodes = %.1f GB; ops %.0f MB per step)" % (
                 rep["nodes_allocated"], rep["nodes_allocated"] * 128 / 1e9, mean_ops * 24 / 1e6),

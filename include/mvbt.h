@@ -254,6 +254,11 @@ int mvbt_batch_plan_create(mvbt_tree* tree, uint64_t max_ops, uint32_t max_batch
                            mvbt_batch_plan** out);
 int mvbt_batch_plan_destroy(mvbt_batch_plan* plan);
 
+/* Launch shape of the plan's persistent path (the autotuner's knobs): tile width 8 or 16 (0 = the
+ * tree's; the node format is the same for both) and resident blocks per SM (-1 = the tree's,
+ * 0 = full occupancy, 6 and 8 pick register-capped kernel variants). Drops a captured graph. */
+int mvbt_batch_plan_set_launch(mvbt_batch_plan* plan, int tile_width, int blocks_per_sm);
+
 /* Runs num_batches batches. batch_off is a HOST array of num_batches + 1 offsets; the op arrays
  * are device arrays. Stream ordered; the call waits for the plan's previous run on `stream`
  * before it reuses the plan's staging memory. MVBT_BATCH_GRAPH re-captures when an array
@@ -354,6 +359,19 @@ int mvbt_serve_trace(mvbt_tree* tree, const mvbt_serve_config* cfg, uint32_t num
                      const uint32_t* key, const uint32_t* arg, const uint64_t* out_off,
                      const uint32_t* range_cap, uint32_t* result, mvbt_pair* range_out,
                      uint64_t* done_ns, uint32_t* snapshot, mvbt_serve_stats* stats);
+
+/* A copy of the tree (all versions, allocator and reclamation state) in a new tree with the same
+ * configuration on the same device. Synchronises the device. The reference shares device
+ * buffers between handle copies instead (include/gpu_versioned_blink_tree.hpp:94-102); a deep
+ * copy has no counterpart there. */
+int mvbt_clone(mvbt_tree* tree, mvbt_tree** out);
+
+/* Checkpoint: writes the tree (configuration, control block, the allocated node prefix of the
+ * pool and the reclamation rings) to a file, and loads such a file into a new tree on `device`
+ * (-1 = current). Both synchronise the device. The reference's pool-image dump is
+ * copy_buffer (include/device_bump_allocator.hpp:71-73), with no load. */
+int mvbt_save(mvbt_tree* tree, const char* path);
+int mvbt_load(const char* path, int device, mvbt_tree** out);
 
 /* Tree kind, tile width and device of a handle. */
 int mvbt_get_info(mvbt_tree* tree, int* kind, int* tile_width, int* device);

@@ -17,7 +17,7 @@ __all__ = [
     "LATEST", "NOT_FOUND", "MVBTError", "lib", "library_path", "gpu_blink_tree",
     "gpu_versioned_btree", "gpu_versioned_blink_tree", "pair_dtype_words", "BatchPlan",
     "BATCH_PERSISTENT", "BATCH_PER_LAUNCH", "BATCH_GRAPH", "NOALLOC_MAX_OPS", "NOALLOC_MAX_BATCHES",
-    "RECLAIM_ALL", "SERVE_SNAPSHOT_PER_BATCH", "SERVE_SNAPSHOT_PER_REQUEST",
+    "RECLAIM_ALL", "SERVE_SNAPSHOT_PER_BATCH", "SERVE_SNAPSHOT_PER_REQUEST", "load",
 ]
 
 LATEST = 0xFFFFFFFF
@@ -105,6 +105,10 @@ _sig("mvbt_batch_plan_kernel_times", ctypes.c_int, _vp, ctypes.POINTER(ctypes.c_
      ctypes.POINTER(_u32))
 _sig("mvbt_stats", ctypes.c_int, _vp, ctypes.POINTER(_u64), _u32)
 _sig("mvbt_reclaim", ctypes.c_int, _vp, _u32, _vp)
+_sig("mvbt_clone", ctypes.c_int, _vp, ctypes.POINTER(_vp))
+_sig("mvbt_save", ctypes.c_int, _vp, ctypes.c_char_p)
+_sig("mvbt_load", ctypes.c_int, ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(_vp))
+_sig("mvbt_batch_plan_set_launch", ctypes.c_int, _vp, ctypes.c_int, ctypes.c_int)
 _sig("mvbt_serve_config_init", None, ctypes.POINTER(mvbt_serve_config))
 _sig("mvbt_serve_trace", ctypes.c_int, _vp, ctypes.POINTER(mvbt_serve_config), _u32, _vp, _vp, _vp, _vp,
      _vp, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.POINTER(mvbt_serve_stats))
@@ -193,6 +197,27 @@ class _TreeBase:
         _check(lib.mvbt_create(self._kind, ctypes.byref(cfg), ctypes.byref(h)), "mvbt_create")
         self._h = h
         self.tile_width = int(tile_width)
+
+    @classmethod
+    def _adopt(cls, handle) -> "_TreeBase":
+        """Wraps a tree handle the library created (clone, load)."""
+        obj = cls.__new__(cls)
+        obj._h = handle
+        kind, w, dev = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _check(lib.mvbt_get_info(handle, ctypes.byref(kind), ctypes.byref(w), ctypes.byref(dev)), "get_info")
+        obj.tile_width = int(w.value)
+        return obj
+
+    def clone(self) -> "_TreeBase":
+        """A copy of the tree (every version, allocator and reclamation state) with the same
+        configuration; changing one leaves the other as it was."""
+        h = _vp()
+        _check(lib.mvbt_clone(self._h, ctypes.byref(h)), "clone")
+        return type(self)._adopt(h)
+
+    def save(self, path) -> None:
+        """Checkpoint of the tree to a file (mvbt_save); load() restores it."""
+        _check(lib.mvbt_save(self._h, str(path).encode()), "save")
 
     # -- lifetime --
     def close(self) -> None:
@@ -415,6 +440,16 @@ class gpu_versioned_btree(_TreeBase):
 
 
 BATCH_PERSISTENT, BATCH_PER_LAUNCH, BATCH_GRAPH = 0, 1, 2
+
+
+def load(path, device: int | None = None):
+    """A tree restored from a file that save() wrote (mvbt_load), as gpu_blink_tree or
+    gpu_versioned_btree."""
+    h = _vp()
+    _check(lib.mvbt_load(str(path).encode(), -1 if device is None else int(device), ctypes.byref(h)), "load")
+    kind = ctypes.c_int()
+    _check(lib.mvbt_get_info(h, ctypes.byref(kind), None, None), "get_info")
+    return (gpu_versioned_btree if kind.value == 1 else gpu_blink_tree)._adopt(h)
 NOALLOC_MAX_OPS, NOALLOC_MAX_BATCHES = 1 << 20, 1024  # MVBT_NOALLOC_MAX_OPS / _BATCHES
 RECLAIM_ALL = 0xFFFFFFFF  # MVBT_RECLAIM_ALL
 SERVE_SNAPSHOT_PER_BATCH, SERVE_SNAPSHOT_PER_REQUEST = 0, 1  # MVBT_SERVE_SNAPSHOT_*
@@ -446,6 +481,12 @@ class BatchPlan:
                                   _ptr(out_off, 8, "out_off"), _ptr(range_cap, name="range_cap"),
                                   _ptr(result, name="result"), _ptr(range_out, 8, "range_out"),
                                   int(mode), _stream(stream)), "batch_run")
+
+    def set_launch(self, tile_width: int = 0, blocks_per_sm: int = -1) -> None:
+        """Launch shape of the persistent path: tile width 8 / 16 (0 = the tree's) and resident
+        blocks per SM (-1 = the tree's, 0 = full occupancy, 6 / 8 = register-capped variants)."""
+        _check(lib.mvbt_batch_plan_set_launch(self._h, int(tile_width), int(blocks_per_sm)), "set_launch")
+        self.launch = (int(tile_width), int(blocks_per_sm))
 
     def enable_timing(self, on: bool = True) -> None:
         """CUDA events around the persistent kernel of each BATCH_PERSISTENT run."""

@@ -49,6 +49,10 @@ struct mvbt_batch_plan {
   bool timing;
   uint32_t timed_runs;
   cudaEvent_t ev_begin[kTimed], ev_end[kTimed];
+  // launch shape of the persistent path (mvbt_batch_plan_set_launch; autotuning): tile width
+  // 0 = the tree's, blocks per SM -1 = the tree's
+  int tile_width       = 0;
+  int blocks_per_sm    = -1;
 };
 
 namespace {
@@ -285,6 +289,19 @@ int enqueue_persistent(mvbt_batch_plan* p, const launch_ctx& c, const batch_view
 
 extern "C" {
 
+int mvbt_batch_plan_set_launch(mvbt_batch_plan* p, int tile_width, int blocks_per_sm) {
+  if (!p) return fail(MVBT_ERR_BAD_ARG, "null plan");
+  if (tile_width != 0 && tile_width != 8 && tile_width != 16) return fail(MVBT_ERR_BAD_ARG, "tile_width must be 0, 8 or 16");
+  if (blocks_per_sm < -1 || blocks_per_sm > 32) return fail(MVBT_ERR_BAD_ARG, "blocks_per_sm must be in [-1, 32]");
+  if (p->have_graph) {
+    cudaGraphExecDestroy(p->graph);
+    p->have_graph = false;
+  }
+  p->tile_width    = tile_width;
+  p->blocks_per_sm = blocks_per_sm;
+  return MVBT_OK;
+}
+
 int mvbt_batch_plan_create(mvbt_tree* tree, uint64_t max_ops, uint32_t max_batches,
                            mvbt_batch_plan** out) {
   if (!tree || !out || max_ops == 0 || max_batches == 0 || max_ops > 0xFFFFFFFFull)
@@ -351,6 +368,8 @@ int mvbt_internal_batch_enqueue(mvbt_batch_plan* p, uint32_t num_batches, const 
   void* ctl;
   int st = mvbt_internal_view(p->tree, &c.view, &c.W, &c.block, &c.sms, &c.bps, &c.maxb, &ctl);
   if (st) return st;
+  if (p->tile_width) c.W = p->tile_width;
+  if (p->blocks_per_sm >= 0) c.bps = (uint32_t)p->blocks_per_sm;
   c.ctl = static_cast<mvbt::control_block*>(ctl);
   for (uint32_t b = num_batches + 1; b <= p->max_batches; ++b) p->h_batch_off[b] = total;
   p->h_params[0] = num_batches;
@@ -382,6 +401,8 @@ int mvbt_batch_run(mvbt_batch_plan* p, uint32_t num_batches, const uint64_t* bat
   void* ctl;
   int st = mvbt_internal_view(p->tree, &c.view, &c.W, &c.block, &c.sms, &c.bps, &c.maxb, &ctl);
   if (st) return st;
+  if (p->tile_width) c.W = p->tile_width;
+  if (p->blocks_per_sm >= 0) c.bps = (uint32_t)p->blocks_per_sm;
   c.ctl = static_cast<mvbt::control_block*>(ctl);
   batch_view B;
   B.type      = type;
@@ -425,6 +446,7 @@ int mvbt_batch_run(mvbt_batch_plan* p, uint32_t num_batches, const uint64_t* bat
   if (mode != MVBT_BATCH_GRAPH) return fail(MVBT_ERR_BAD_ARG, "unknown batch mode");
 
   const void* key_now[8] = {type, key, arg, out_off, range_cap, result, range_out, stream};
+  // (a change of launch shape drops the captured graph: mvbt_batch_plan_set_launch)
   if (!p->have_graph || std::memcmp(key_now, p->graph_key, sizeof(key_now)) != 0) {
     if (p->have_graph) {
       cudaGraphExecDestroy(p->graph);

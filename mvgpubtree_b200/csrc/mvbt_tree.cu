@@ -400,6 +400,191 @@ int mvbt_get_info(mvbt_tree* t, int* kind, int* tile_width, int* device) {
   return MVBT_OK;
 }
 
+// ---- copies of a tree: clone on the device, image files for checkpoints ----
+static mvbt_config config_of(const mvbt_tree* t) {
+  mvbt_config c;
+  mvbt_config_init(&c);
+  c.pool_bytes    = t->capacity * 128;
+  c.device        = t->device;
+  c.tile_width    = t->tile_width;
+  c.block_size    = t->block_size;
+  c.spin_limit    = t->spin_limit;
+  c.chunk_nodes   = t->chunk;
+  c.blocks_per_sm = t->blocks_per_sm;
+  c.max_blocks    = t->max_blocks;
+  c.wait_ms       = t->wait_ms;
+  c.reclaim       = t->retire_log ? 1u : 0u;
+  return c;
+}
+
+static uint64_t pow2_at_least(uint64_t x) {
+  uint64_t p = 1;
+  while (p < x) p <<= 1;
+  return p;
+}
+
+// Retire log and free ring sizes of a tree created with reclamation (as mvbt_create makes them).
+static void ring_sizes(const mvbt_tree* t, uint64_t* log_cap, uint64_t* ring_cap) {
+  *log_cap  = t->retire_log ? pow2_at_least(t->capacity) : 0;
+  *ring_cap = t->retire_log ? pow2_at_least(t->capacity + (uint64_t)mvbt::kMaxSmSlots * t->chunk) : 0;
+}
+
+// Writes the control block image `c` into tree t, keeping t's own ring addresses.
+static int put_control(mvbt_tree* t, control_block c) {
+  c.retire_log = (unsigned long long)t->retire_log;
+  c.free_ring  = (unsigned long long)t->free_ring;
+  MVBT_CUDA_TRY(cudaMemcpy(t->ctl, &c, sizeof(c), cudaMemcpyHostToDevice));
+  return MVBT_OK;
+}
+
+int mvbt_clone(mvbt_tree* src, mvbt_tree** out) {
+  if (!src || !out) return fail(MVBT_ERR_BAD_ARG, "null argument");
+  *out = nullptr;
+  MVBT_CUDA_TRY(cudaSetDevice(src->device));
+  MVBT_CUDA_TRY(cudaDeviceSynchronize());
+  const mvbt_config cfg = config_of(src);
+  mvbt_tree* t          = nullptr;
+  int st                = mvbt_create(src->kind, &cfg, &t);
+  if (st) return st;
+  control_block c;
+  cudaError_t e = cudaMemcpy(&c, src->ctl, sizeof(c), cudaMemcpyDeviceToHost);
+  const uint64_t nodes = std::min<uint64_t>(c.bump, src->capacity);
+  uint64_t log_cap = 0, ring_cap = 0;
+  ring_sizes(src, &log_cap, &ring_cap);
+  if (e == cudaSuccess) e = cudaMemcpy(t->pool, src->pool, nodes * 128, cudaMemcpyDeviceToDevice);
+  if (e == cudaSuccess && log_cap) e = cudaMemcpy(t->retire_log, src->retire_log, log_cap * 4, cudaMemcpyDeviceToDevice);
+  if (e == cudaSuccess && ring_cap) e = cudaMemcpy(t->free_ring, src->free_ring, ring_cap * 4, cudaMemcpyDeviceToDevice);
+  if (e != cudaSuccess) {
+    mvbt_destroy(t);
+    return fail(MVBT_ERR_CUDA, std::string("clone: ") + cudaGetErrorString(e));
+  }
+  st = put_control(t, c);
+  if (st) {
+    mvbt_destroy(t);
+    return st;
+  }
+  *out = t;
+  return MVBT_OK;
+}
+
+namespace {
+struct image_header {
+  char magic[8];            // "MVBTIMG1"
+  uint32_t version;         // 1
+  int32_t kind;
+  uint64_t capacity;        // nodes
+  int32_t tile_width, block_size;
+  uint32_t spin_limit, chunk, blocks_per_sm, max_blocks, wait_ms, reclaim;
+  uint64_t nodes;           // node image length (the allocated prefix of the pool)
+  uint64_t control_bytes;   // sizeof(control_block) of the writer
+  uint64_t log_cap, ring_cap;
+};
+constexpr uint64_t kIoChunk = 64ull << 20;
+
+// Copies `bytes` between a file and device memory through a pinned staging buffer.
+int device_file_copy(FILE* f, void* dev, uint64_t bytes, bool to_file, void* stage) {
+  for (uint64_t done = 0; done < bytes; done += kIoChunk) {
+    const uint64_t n = std::min(kIoChunk, bytes - done);
+    if (to_file) {
+      MVBT_CUDA_TRY(cudaMemcpy(stage, (char*)dev + done, n, cudaMemcpyDeviceToHost));
+      if (std::fwrite(stage, 1, n, f) != n) return fail(MVBT_ERR_BAD_ARG, "tree image: write failed");
+    } else {
+      if (std::fread(stage, 1, n, f) != n) return fail(MVBT_ERR_BAD_ARG, "tree image: file is truncated");
+      MVBT_CUDA_TRY(cudaMemcpy((char*)dev + done, stage, n, cudaMemcpyHostToDevice));
+    }
+  }
+  return MVBT_OK;
+}
+}  // namespace
+
+int mvbt_save(mvbt_tree* t, const char* path) {
+  if (!t || !path) return fail(MVBT_ERR_BAD_ARG, "null argument");
+  MVBT_CUDA_TRY(cudaSetDevice(t->device));
+  MVBT_CUDA_TRY(cudaDeviceSynchronize());
+  control_block c;
+  MVBT_CUDA_TRY(cudaMemcpy(&c, t->ctl, sizeof(c), cudaMemcpyDeviceToHost));
+  image_header h;
+  std::memset(&h, 0, sizeof(h));
+  std::memcpy(h.magic, "MVBTIMG1", 8);
+  h.version = 1;
+  h.kind    = t->kind;
+  h.capacity = t->capacity;
+  h.tile_width = t->tile_width;
+  h.block_size = t->block_size;
+  h.spin_limit = t->spin_limit;
+  h.chunk = t->chunk;
+  h.blocks_per_sm = t->blocks_per_sm;
+  h.max_blocks = t->max_blocks;
+  h.wait_ms = t->wait_ms;
+  h.reclaim = t->retire_log ? 1u : 0u;
+  h.nodes = std::min<uint64_t>(c.bump, t->capacity);
+  h.control_bytes = sizeof(control_block);
+  ring_sizes(t, &h.log_cap, &h.ring_cap);
+  FILE* f = std::fopen(path, "wb");
+  if (!f) return fail(MVBT_ERR_BAD_ARG, std::string("cannot open ") + path);
+  void* stage = nullptr;
+  int st = MVBT_OK;
+  if (cudaMallocHost(&stage, kIoChunk) != cudaSuccess) st = fail(MVBT_ERR_OUT_OF_MEMORY, "pinned staging");
+  if (!st && (std::fwrite(&h, sizeof(h), 1, f) != 1 || std::fwrite(&c, sizeof(c), 1, f) != 1))
+    st = fail(MVBT_ERR_BAD_ARG, "tree image: write failed");
+  if (!st) st = device_file_copy(f, t->pool, h.nodes * 128, true, stage);
+  if (!st && h.log_cap) st = device_file_copy(f, t->retire_log, h.log_cap * 4, true, stage);
+  if (!st && h.ring_cap) st = device_file_copy(f, t->free_ring, h.ring_cap * 4, true, stage);
+  if (stage) cudaFreeHost(stage);
+  if (std::fclose(f) != 0 && !st) st = fail(MVBT_ERR_BAD_ARG, "tree image: close failed");
+  return st;
+}
+
+int mvbt_load(const char* path, int device, mvbt_tree** out) {
+  if (!path || !out) return fail(MVBT_ERR_BAD_ARG, "null argument");
+  *out    = nullptr;
+  FILE* f = std::fopen(path, "rb");
+  if (!f) return fail(MVBT_ERR_BAD_ARG, std::string("cannot open ") + path);
+  image_header h;
+  control_block c;
+  if (std::fread(&h, sizeof(h), 1, f) != 1 || std::memcmp(h.magic, "MVBTIMG1", 8) != 0 || h.version != 1 ||
+      h.control_bytes != sizeof(control_block) || std::fread(&c, sizeof(c), 1, f) != 1) {
+    std::fclose(f);
+    return fail(MVBT_ERR_BAD_ARG, "not a tree image of this library version");
+  }
+  mvbt_config cfg;
+  mvbt_config_init(&cfg);
+  cfg.pool_bytes    = h.capacity * 128;
+  cfg.device        = device;
+  cfg.tile_width    = h.tile_width;
+  cfg.block_size    = h.block_size;
+  cfg.spin_limit    = h.spin_limit;
+  cfg.chunk_nodes   = h.chunk;
+  cfg.blocks_per_sm = h.blocks_per_sm;
+  cfg.max_blocks    = h.max_blocks;
+  cfg.wait_ms       = h.wait_ms;
+  cfg.reclaim       = h.reclaim;
+  mvbt_tree* t      = nullptr;
+  int st            = mvbt_create(h.kind, &cfg, &t);
+  if (st) {
+    std::fclose(f);
+    return st;
+  }
+  uint64_t log_cap = 0, ring_cap = 0;
+  ring_sizes(t, &log_cap, &ring_cap);
+  if (h.nodes > t->capacity || log_cap != h.log_cap || ring_cap != h.ring_cap)
+    st = fail(MVBT_ERR_BAD_ARG, "tree image does not match the tree it configures");
+  void* stage = nullptr;
+  if (!st && cudaMallocHost(&stage, kIoChunk) != cudaSuccess) st = fail(MVBT_ERR_OUT_OF_MEMORY, "pinned staging");
+  if (!st) st = device_file_copy(f, t->pool, h.nodes * 128, false, stage);
+  if (!st && log_cap) st = device_file_copy(f, t->retire_log, log_cap * 4, false, stage);
+  if (!st && ring_cap) st = device_file_copy(f, t->free_ring, ring_cap * 4, false, stage);
+  if (stage) cudaFreeHost(stage);
+  std::fclose(f);
+  if (!st) st = put_control(t, c);
+  if (st) {
+    mvbt_destroy(t);
+    return st;
+  }
+  *out = t;
+  return MVBT_OK;
+}
+
 int mvbt_insert(mvbt_tree* t, const uint32_t* keys, const uint32_t* values, uint32_t n, void* stream,
                 int in_place) {
   (void)in_place;  // both reference variants keep every snapshot-visible version
