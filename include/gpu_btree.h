@@ -147,6 +147,14 @@ class gpu_blink_tree : public detail::tree_base<Key, Value, MVBT_KIND_BLINK> {
   using typename base::pair_type;
   using typename base::size_type;
   explicit gpu_blink_tree(const mvbt_config* cfg = nullptr) : base(cfg) {}
+  // reference: the bulk-build constructor (gpu_blink_tree.hpp:85-136): sorted input only, a
+  // half-full tree; unsorted input throws (the reference prints and terminates)
+  gpu_blink_tree(const Key* keys, const Value* values, size_type num_keys, bool sorted_input = false,
+                 cudaStream_t stream = 0, const mvbt_config* cfg = nullptr)
+      : base(cfg) {
+    if (!sorted_input) throw mvbt_error(MVBT_ERR_BAD_ARG, "bulk build: only sorted input is supported");
+    base::check(mvbt_bulk_build(this->tree_.get(), keys, values, num_keys, 8, stream), "bulk_build");
+  }
   // reference: range_query (gpu_blink_tree.hpp:247-265)
   void range_query(const Key* lower_bound, const Key* upper_bound, pair_type* result,
                    size_type* counts, size_type average_range_length, size_type num_keys,

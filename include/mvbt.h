@@ -360,6 +360,17 @@ int mvbt_serve_trace(mvbt_tree* tree, const mvbt_serve_config* cfg, uint32_t num
                      const uint32_t* range_cap, uint32_t* result, mvbt_pair* range_out,
                      uint64_t* done_ns, uint32_t* snapshot, mvbt_serve_stats* stats);
 
+/* Builds a fresh tree (no writes or snapshots yet) from n pairs with keys sorted strictly
+ * increasing (device arrays; key 0xFFFFFFFF is not allowed; a key 0 replaces the tombstone's
+ * value). Every node is written once: leaves hold `fill` pairs and interior nodes `fill`
+ * children (0 = 8, half full as the reference builds, so later inserts do not split at once;
+ * at most 13). Checks the order on the device first (MVBT_ERR_BAD_ARG if unsorted); synchronises
+ * the stream. Works for both tree kinds.
+ * Replaces: the bulk-build constructor gpu_blink_tree(keys, values, n, sorted_input, stream)
+ * (include/gpu_blink_tree.hpp:85-136, include/btree_kernels.hpp:915-1025). */
+int mvbt_bulk_build(mvbt_tree* tree, const uint32_t* keys, const uint32_t* values, uint64_t n,
+                    uint32_t fill, void* stream);
+
 /* A copy of the tree (all versions, allocator and reclamation state) in a new tree with the same
  * configuration on the same device. Synchronises the device. The reference shares device
  * buffers between handle copies instead (include/gpu_versioned_blink_tree.hpp:94-102); a deep

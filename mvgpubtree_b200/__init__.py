@@ -106,6 +106,7 @@ _sig("mvbt_batch_plan_kernel_times", ctypes.c_int, _vp, ctypes.POINTER(ctypes.c_
 _sig("mvbt_stats", ctypes.c_int, _vp, ctypes.POINTER(_u64), _u32)
 _sig("mvbt_reclaim", ctypes.c_int, _vp, _u32, _vp)
 _sig("mvbt_clone", ctypes.c_int, _vp, ctypes.POINTER(_vp))
+_sig("mvbt_bulk_build", ctypes.c_int, _vp, _P, _P, _u64, _u32, _vp)
 _sig("mvbt_save", ctypes.c_int, _vp, ctypes.c_char_p)
 _sig("mvbt_load", ctypes.c_int, ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(_vp))
 _sig("mvbt_batch_plan_set_launch", ctypes.c_int, _vp, ctypes.c_int, ctypes.c_int)
@@ -207,6 +208,14 @@ class _TreeBase:
         _check(lib.mvbt_get_info(handle, ctypes.byref(kind), ctypes.byref(w), ctypes.byref(dev)), "get_info")
         obj.tile_width = int(w.value)
         return obj
+
+    def bulk_build(self, keys, values, num_keys: int | None = None, fill: int = 0, stream=None) -> None:
+        """Builds this fresh tree from pairs with keys sorted strictly increasing (device tensors);
+        leaves hold `fill` pairs (0 = 8, half full, as the reference's bulk-build constructor,
+        include/gpu_blink_tree.hpp:85-136)."""
+        n = _numel(keys) if num_keys is None else int(num_keys)
+        _check(lib.mvbt_bulk_build(self._h, _ptr(keys, name="keys"), _ptr(values, name="values"), n,
+                                   int(fill), _stream(stream)), "bulk_build")
 
     def clone(self) -> "_TreeBase":
         """A copy of the tree (every version, allocator and reclamation state) with the same

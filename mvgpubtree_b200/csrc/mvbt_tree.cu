@@ -400,6 +400,131 @@ int mvbt_get_info(mvbt_tree* t, int* kind, int* tile_width, int* device) {
   return MVBT_OK;
 }
 
+// ---- bulk build from sorted pairs ----
+// Entry e of the built tree: the tombstone {0, 0} first unless the input starts with key 0 (its
+// value then replaces the tombstone's), then the input pairs in order.
+struct bulk_input {
+  const uint32_t* keys;
+  const uint32_t* values;
+  uint32_t off;  // 1: entry 0 is the tombstone; 0: the input holds key 0
+  uint64_t m;    // entries
+  __device__ uint32_t key(uint64_t e) const { return (off && e == 0) ? 0u : keys[e - off]; }
+  __device__ uint32_t value(uint64_t e) const { return (off && e == 0) ? 0u : values[e - off]; }
+};
+struct bulk_levels {
+  uint32_t n;                 // levels, leaves = level 0
+  uint32_t fill;              // pairs per leaf = children per interior node
+  uint64_t base[mvbt::kMaxLevels];   // first node index of each level
+  uint64_t count[mvbt::kMaxLevels];  // nodes of each level
+  uint64_t span[mvbt::kMaxLevels];   // entries under one node of each level (fill^(level+1), saturated)
+};
+
+// Sorted strictly increasing, no 0xFFFFFFFF: otherwise sets *bad.
+__global__ void k_bulk_check(const uint32_t* keys, uint64_t n, uint32_t* bad) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t k = keys[i];
+    if (k == mvbt::kEmptyKey || (i + 1 < n && keys[i + 1] <= k)) atomicOr(bad, 1u);
+  }
+}
+
+// One warp per node, lane w writes word w: pairs 0..12, then {low, mod}, {high, link}, {ts, level|older}.
+__global__ void k_bulk_build(uint32_t* pool, bulk_input in, bulk_levels L, uint64_t total) {
+  const uint32_t w                = threadIdx.x & 31u;
+  const uint64_t warps            = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t g = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; g < total; g += warps) {
+    uint32_t l = 0;
+    while (l + 1 < L.n && g >= L.base[l + 1] - L.base[0]) ++l;
+    const uint64_t j     = g - (L.base[l] - L.base[0]);
+    const uint64_t first = j * L.span[l];                     // first entry under this node
+    const uint64_t child_span = l ? L.span[l - 1] : 1;        // entries under one child (leaf: 1)
+    uint64_t items = l ? L.count[l - 1] - j * L.fill : in.m - first;  // children or entries left
+    if (items > L.fill) items = L.fill;
+    uint32_t v = mvbt::kEmptyKey;
+    if (w < 2 * mvbt::kDataPairs) {
+      const uint64_t p = w >> 1;
+      if (p < items) {
+        const uint64_t e = first + p * child_span;
+        if (l == 0) v = (w & 1) ? in.value(e) : in.key(e);
+        else v = (w & 1) ? (uint32_t)(L.base[l - 1] + j * L.fill + p) : in.key(e);
+      }
+    } else if (w == 26) {
+      v = in.key(first);
+    } else if (w == 27) {
+      v = 0;  // modification count
+    } else if (w == 28) {
+      const uint64_t next = first + L.span[l];
+      v = (j + 1 < L.count[l] && next < in.m) ? in.key(next) : mvbt::kEmptyKey;
+    } else if (w == 29) {
+      v = (j + 1 < L.count[l]) ? (uint32_t)(L.base[l] + j + 1) : mvbt::kNone;
+    } else if (w == 30) {
+      v = 0;  // ts
+    } else {
+      v = (l << 28) | mvbt::kNone;
+    }
+    pool[(L.base[l] + j) * 32 + w] = v;
+  }
+}
+
+// The anchor {0 -> top}, one level above the top; the bump pointer past the built nodes.
+__global__ void k_bulk_anchor(uint32_t* pool, control_block* c, uint32_t top, uint32_t top_level, uint32_t bump) {
+  const uint32_t w = threadIdx.x;
+  if (w >= 32) return;
+  uint32_t v = mvbt::kEmptyKey;
+  if (w == 0) v = 0;
+  else if (w == 1) v = top;
+  else if (w == 26 || w == 27 || w == 30) v = 0;
+  else if (w == 29) v = mvbt::kNone;
+  else if (w == 31) v = ((top_level + 1) << 28) | mvbt::kNone;
+  pool[w] = v;
+  if (w == 0) c->bump = bump;
+}
+
+int mvbt_bulk_build(mvbt_tree* t, const uint32_t* keys, const uint32_t* values, uint64_t n, uint32_t fill,
+                    void* stream) {
+  if (!t || (n && (!keys || !values))) return fail(MVBT_ERR_BAD_ARG, "null argument");
+  if (fill == 0) fill = 8;
+  if (fill < 2 || fill > (uint32_t)mvbt::kDataPairs) return fail(MVBT_ERR_BAD_ARG, "fill must be in [2, 13]");
+  MVBT_CUDA_TRY(cudaSetDevice(t->device));
+  cudaStream_t s = as_stream(stream);
+  MVBT_CUDA_TRY(cudaStreamSynchronize(s));
+  control_block c;
+  MVBT_CUDA_TRY(cudaMemcpy(&c, t->ctl, sizeof(c), cudaMemcpyDeviceToHost));
+  uint32_t leaf[4] = {0, 0, 0, 0};  // the first leaf's first two pairs
+  MVBT_CUDA_TRY(cudaMemcpy(leaf, t->pool + 32 * mvbt::kFirstLeaf, sizeof(leaf), cudaMemcpyDeviceToHost));
+  if (c.bump != (uint32_t)mvbt::kInitialNodes || c.epoch != 0 || leaf[2] != mvbt::kEmptyKey)
+    return fail(MVBT_ERR_BAD_ARG, "bulk build needs a fresh tree (no writes, no snapshots)");
+  if (n == 0) return MVBT_OK;
+  uint32_t first_key = 0;
+  MVBT_CUDA_TRY(cudaMemcpy(&first_key, keys, 4, cudaMemcpyDeviceToHost));
+  MVBT_CUDA_TRY(cudaMemsetAsync(t->d_words, 0, 4, s));
+  k_bulk_check<<<(unsigned)std::min<uint64_t>((n + 255) / 256, 4096), 256, 0, s>>>(keys, n, t->d_words);
+  MVBT_CUDA_TRY(cudaMemcpyAsync(t->h_word, t->d_words, 4, cudaMemcpyDeviceToHost, s));
+  MVBT_CUDA_TRY(cudaStreamSynchronize(s));
+  if (*t->h_word) return fail(MVBT_ERR_BAD_ARG, "bulk build needs keys sorted strictly increasing, without 0xFFFFFFFF");
+  bulk_input in{keys, values, first_key == 0 ? 0u : 1u, n + (first_key == 0 ? 0 : 1)};
+  bulk_levels L{};
+  L.fill = fill;
+  uint64_t count = (in.m + fill - 1) / fill, base = 1, span = fill, total = 0;
+  for (;;) {
+    if (L.n >= (uint32_t)mvbt::kMaxLevels - 1) return fail(MVBT_ERR_BAD_ARG, "bulk build: tree too tall");
+    L.base[L.n]  = base;
+    L.count[L.n] = count;
+    L.span[L.n]  = span;
+    ++L.n;
+    base += count;
+    total += count;
+    if (count == 1) break;
+    count = (count + fill - 1) / fill;
+    span  = span > (~0ull) / fill ? ~0ull : span * fill;
+  }
+  if (1 + total > t->capacity) return fail(MVBT_ERR_POOL_EXHAUSTED, "bulk build: the pool is too small");
+  const uint64_t threads = total * 32;
+  const unsigned grid    = (unsigned)std::min<uint64_t>((threads + 255) / 256, (uint64_t)t->num_sms * 64);
+  k_bulk_build<<<grid, 256, 0, s>>>(t->pool, in, L, total);
+  k_bulk_anchor<<<1, 32, 0, s>>>(t->pool, t->ctl, (uint32_t)L.base[L.n - 1], L.n - 1, (uint32_t)(1 + total));
+  return check_launch();
+}
+
 // ---- copies of a tree: clone on the device, image files for checkpoints ----
 static mvbt_config config_of(const mvbt_tree* t) {
   mvbt_config c;
