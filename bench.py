@@ -10,8 +10,9 @@ for this workload); each step gets fresh batches, generated against the evolving
 
 value    : Mops/s of the batched path (one persistent launch per step, ops resident in HBM).
 e2e      : Mops/s through the public batch API with host buffers: per step the op arrays are
-           copied from pinned host memory, the captured CUDA graph is replayed and the results
-           (values, counts and range-output slots) are copied back.
+           copied from pinned host memory, the captured CUDA graph is replayed, and the results
+           (values, counts) and the range pairs that exist (packed on the device) are copied
+           back; two steps are in flight, so copies overlap the next step's run.
 plain    : the same batches as one snapshot + one launch per batch (the drop-in method).
 roofline : algorithmic bytes of the persistent kernel per launch / its CUDA-event time.
 serving  : continuous batching of Poisson-arriving requests (lognormal sizes, median 256 ops) at
@@ -63,7 +64,7 @@ def parse_args():
     ap.add_argument("--blocks-per-sm", type=int, default=0,
                     help="0 = full occupancy of the default kernel; 6 / 8 = register-capped variants")
     ap.add_argument("--plain-steps", type=int, default=2)
-    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=4)
     ap.add_argument("--pool-gb", type=float, default=24.0)
     ap.add_argument("--cpu-sample-ops", type=int, default=4_000_000,
                     help="ops of the bounded CPU-baseline sample per step")
@@ -218,7 +219,7 @@ def run_ours(args, dist: Dist):
     seed = args.seed + 7919 * dist.rank
     W, K = max(3, args.warmup), args.steps
     Wp, Kp = 1, max(1, args.plain_steps)
-    We, Ke = 1, max(1, args.e2e_steps)
+    We, Ke = 2, max(1, args.e2e_steps)  # e2e warm-up: one step per buffer set (graph capture, scratch)
     n_steps = max(W + K, Wp + Kp) + We + Ke
     init, vals, steps, gen_s = make_workload(seed, args.initial_keys, n_steps, args.batches)
 
@@ -299,35 +300,74 @@ def run_ours(args, dist: Dist):
     del dsteps, results
     torch.cuda.empty_cache()
 
-    # ---- e2e: public API with pinned host buffers, CUDA graph replay ----
+    # ---- e2e: public API with pinned host buffers, CUDA graph replay, two steps in flight ----
+    # Step s: its op arrays cross on the input stream, its graph replay and the packing of its
+    # range pairs run on the compute stream, and its results and packed pairs cross back on the
+    # output stream once the host has its pair count, while step s + 1 runs. Buffers and plans
+    # alternate between two sets.
     e2e_steps = steps[max(W + K, Wp + Kp):]
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.int64 if a.dtype == np.uint64 else np.int32)).pin_memory()
-    d_ops = [torch.empty(max_ops, dtype=torch.int32, device="cuda") for _ in range(3)]
-    d_off = torch.empty(max_ops, dtype=torch.int64, device="cuda")
-    d_cap = torch.empty(max_ops, dtype=torch.int32, device="cuda")
-    d_res = torch.empty(max_ops, dtype=torch.int32, device="cuda")
-    h_res = torch.empty(max_ops, dtype=torch.int32).pin_memory()
-    h_rout = torch.empty(max(1, max_pairs) * 2, dtype=torch.int32).pin_memory()
+    bufs = []
+    for k in range(2):
+        bp = plan if k == 0 else trees["batched"].batch_plan(max_ops, args.batches)
+        if k and tune:
+            bp.set_launch(tune["tile_width"], tune["blocks_per_sm"])
+        bufs.append({
+            "ops": [torch.empty(max_ops, dtype=torch.int32, device="cuda") for _ in range(3)],
+            "off": torch.empty(max_ops, dtype=torch.int64, device="cuda"),
+            "cap": torch.empty(max_ops, dtype=torch.int32, device="cuda"),
+            "res": torch.empty(max_ops, dtype=torch.int32, device="cuda"),
+            "rout": range_out if k == 0 else torch.empty(max(1, max_pairs) * 2, dtype=torch.int32, device="cuda"),
+            "comp": torch.empty(max(1, max_pairs) * 2, dtype=torch.int32, device="cuda"),
+            "h_res": torch.empty(max_ops, dtype=torch.int32).pin_memory(),
+            "h_comp": torch.empty(max(1, max_pairs) * 2, dtype=torch.int32).pin_memory(),
+            "plan": bp, "ev_in": torch.cuda.Event(), "ev_k": torch.cuda.Event(), "ev_out": torch.cuda.Event()})
     h_in = [[pin(b.type), pin(b.key), pin(b.arg), pin(b.out_off), pin(b.range_cap)] for b in e2e_steps]
+    h_total = torch.zeros(len(e2e_steps), dtype=torch.int64).pin_memory()
+    s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream()
+
+    def finish(q):
+        bq, b = bufs[q % 2], e2e_steps[q]
+        bq["ev_k"].synchronize()  # step q's run and packing are done; its pair count is on the host
+        tot = int(h_total[q])
+        with torch.cuda.stream(s_out):
+            s_out.wait_event(bq["ev_k"])
+            bq["h_res"][: b.num_ops].copy_(bq["res"][: b.num_ops], non_blocking=True)
+            bq["h_comp"][: 2 * tot].copy_(bq["comp"][: 2 * tot], non_blocking=True)
+            bq["ev_out"].record(s_out)
+        return b.num_ops * 4 + 8 + tot * 8
+
     h2d = d2h = 0
-    e2e_ms = 0.0
     for s, b in enumerate(e2e_steps):
-        n = b.num_ops
+        bs, n = bufs[s % 2], b.num_ops
         if s == We:
+            if s:
+                finish(s - 1)
             dist.barrier()
             torch.cuda.synchronize()
             ev0.record(stream)
-        dst = [d_ops[0][:n], d_ops[1][:n], d_ops[2][:n], d_off[:n], d_cap[:n]]
-        for d, h in zip(dst, h_in[s]):
-            d.copy_(h, non_blocking=True)
-        plan.run(b.batch_off, d_ops[0], d_ops[1], d_ops[2], d_off, d_cap, d_res, range_out,
-                 mode=mv.BATCH_GRAPH, stream=stream)
-        h_res[:n].copy_(d_res[:n], non_blocking=True)
-        h_rout[: 2 * b.range_pairs].copy_(range_out[: 2 * b.range_pairs], non_blocking=True)
+        with torch.cuda.stream(s_in):
+            s_in.wait_event(bs["ev_k"])  # the run two steps back has read these buffers
+            dst = [bs["ops"][0][:n], bs["ops"][1][:n], bs["ops"][2][:n], bs["off"][:n], bs["cap"][:n]]
+            for d, h in zip(dst, h_in[s]):
+                d.copy_(h, non_blocking=True)
+            bs["ev_in"].record(s_in)
+        stream.wait_event(bs["ev_in"])
+        stream.wait_event(bs["ev_out"])  # its results from two steps back have crossed
+        bs["plan"].run(b.batch_off, bs["ops"][0], bs["ops"][1], bs["ops"][2], bs["off"], bs["cap"], bs["res"],
+                       bs["rout"], mode=mv.BATCH_GRAPH, stream=stream)
+        # the pair count goes straight to pinned host memory: no copy queued behind the big ones
+        bs["plan"].compact_ranges(n, bs["ops"][0], bs["res"], bs["off"], bs["cap"], bs["rout"], bs["comp"],
+                                  h_total[s:s + 1], stream=stream)
+        bs["ev_k"].record(stream)
         if s >= We:
             h2d += sum(int(h.numel() * h.element_size()) for h in h_in[s])
-            d2h += n * 4 + b.range_pairs * 8
-    ev1.record(stream)
+        if s >= 1 and s != We:
+            out_bytes = finish(s - 1)
+            if s - 1 >= We:
+                d2h += out_bytes
+    d2h += finish(len(e2e_steps) - 1)
+    ev1.record(s_out)
     torch.cuda.synchronize()
     trees["batched"].check_errors()
     e2e_ms = dist.max(ev0.elapsed_time(ev1))
@@ -377,7 +417,9 @@ def run_ours(args, dist: Dist):
                             "batched_over_plain": round(value / plain_value, 3)},
         "e2e": {"value": round(e2e_value, 2), "unit": UNIT,
                 "h2d_bytes_per_step": int(h2d / max(1, Ke)), "d2h_bytes_per_step": int(d2h / max(1, Ke)),
-                "mode": "CUDA graph replay via the public batch API, pinned host buffers"},
+                "mode": "CUDA graph replay via the public batch API, pinned host buffers, two steps in "
+                        "flight: op arrays in, results and the range pairs that exist (packed by "
+                        "mvbt_batch_compact_ranges) back, overlapping the next step's run"},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": traffic,
                      "kernel": "k_batched", "kernel_ms": round(avg_kms, 3),
@@ -386,7 +428,7 @@ def run_ours(args, dist: Dist):
         "gpu_launches": 5 * K,
     }
     if args.serve_loads:
-        del plans, pplan, plan, d_ops, d_off, d_cap, d_res, h_res, h_rout, h_in, range_out
+        del plans, pplan, plan, bufs, h_in, range_out
         trees.clear()
         torch.cuda.empty_cache()
         out["serving"] = run_serving(args, seed, init, vals, dev)

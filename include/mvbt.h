@@ -254,15 +254,27 @@ int mvbt_batch_plan_create(mvbt_tree* tree, uint64_t max_ops, uint32_t max_batch
                            mvbt_batch_plan** out);
 int mvbt_batch_plan_destroy(mvbt_batch_plan* plan);
 
+/* Compact range output of a batch run (device arrays, stream-ordered, uses the plan's scratch,
+ * which the first call allocates): the first min(result[i], range_cap[i]) pairs of every range
+ * query i, in op order, packed into `compact` (room for the sum of the range caps), and the number
+ * of pairs written to *total (a device uint64). Query i's pairs start at the sum of
+ * min(count, cap) over the range queries before it, which the caller recomputes from result[] and
+ * range_cap[]. A caller that copies results to the host then copies only the pairs that exist
+ * instead of every fixed-size slot. */
+int mvbt_batch_compact_ranges(mvbt_batch_plan* plan, uint64_t num_ops, const uint32_t* type,
+                              const uint32_t* result, const uint64_t* out_off, const uint32_t* range_cap,
+                              const mvbt_pair* range_out, mvbt_pair* compact, uint64_t* total, void* stream);
+
 /* Launch shape of the plan's persistent path (the autotuner's knobs): tile width 8 or 16 (0 = the
  * tree's; the node format is the same for both) and resident blocks per SM (-1 = the tree's,
  * 0 = full occupancy, 6 and 8 pick register-capped kernel variants). Drops a captured graph. */
 int mvbt_batch_plan_set_launch(mvbt_batch_plan* plan, int tile_width, int blocks_per_sm);
 
 /* Runs num_batches batches. batch_off is a HOST array of num_batches + 1 offsets; the op arrays
- * are device arrays. Stream ordered; the call waits for the plan's previous run on `stream`
- * before it reuses the plan's staging memory. MVBT_BATCH_GRAPH re-captures when an array
- * pointer or the stream changes. */
+ * are device arrays. Stream ordered; the call waits (on the host) for the plan's own previous
+ * persistent or graph run to finish before it reuses the plan's pinned staging memory, so a
+ * caller can keep other plans and streams busy meanwhile. MVBT_BATCH_GRAPH re-captures when an
+ * array pointer or the stream changes. */
 int mvbt_batch_run(mvbt_batch_plan* plan, uint32_t num_batches, const uint64_t* batch_off,
                    const uint32_t* type, const uint32_t* key, const uint32_t* arg,
                    const uint64_t* out_off, const uint32_t* range_cap, uint32_t* result,

@@ -110,6 +110,7 @@ _sig("mvbt_bulk_build", ctypes.c_int, _vp, _P, _P, _u64, _u32, _vp)
 _sig("mvbt_save", ctypes.c_int, _vp, ctypes.c_char_p)
 _sig("mvbt_load", ctypes.c_int, ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(_vp))
 _sig("mvbt_batch_plan_set_launch", ctypes.c_int, _vp, ctypes.c_int, ctypes.c_int)
+_sig("mvbt_batch_compact_ranges", ctypes.c_int, _vp, _u64, _P, _P, _P, _P, _P, _P, _P, _vp)
 _sig("mvbt_serve_config_init", None, ctypes.POINTER(mvbt_serve_config))
 _sig("mvbt_serve_trace", ctypes.c_int, _vp, ctypes.POINTER(mvbt_serve_config), _u32, _vp, _vp, _vp, _vp,
      _vp, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.POINTER(mvbt_serve_stats))
@@ -490,6 +491,18 @@ class BatchPlan:
                                   _ptr(out_off, 8, "out_off"), _ptr(range_cap, name="range_cap"),
                                   _ptr(result, name="result"), _ptr(range_out, 8, "range_out"),
                                   int(mode), _stream(stream)), "batch_run")
+
+    def compact_ranges(self, num_ops: int, type, result, out_off, range_cap, range_out, compact, total,
+                       stream=None) -> None:
+        """Packs the first min(count, cap) pairs of every range query, in op order, into `compact`
+        (a CUDA tensor or pinned host memory, which the kernel then writes directly) and the pair
+        count into `total` (one 64-bit word). Query i's pairs start at the sum of min(count, cap)
+        over the range queries before it."""
+        _check(lib.mvbt_batch_compact_ranges(self._h, int(num_ops), _ptr(type, name="type"),
+                                             _ptr(result, name="result"), _ptr(out_off, 8, "out_off"),
+                                             _ptr(range_cap, name="range_cap"), _ptr(range_out, 8, "range_out"),
+                                             _ptr(compact, 8, "compact"), _ptr(total, 8, "total"),
+                                             _stream(stream)), "compact_ranges")
 
     def set_launch(self, tile_width: int = 0, blocks_per_sm: int = -1) -> None:
         """Launch shape of the persistent path: tile width 8 / 16 (0 = the tree's) and resident

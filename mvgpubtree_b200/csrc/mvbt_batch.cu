@@ -53,6 +53,12 @@ struct mvbt_batch_plan {
   // 0 = the tree's, blocks per SM -1 = the tree's
   int tile_width       = 0;
   int blocks_per_sm    = -1;
+  // scratch of mvbt_batch_compact_ranges (grown on demand)
+  void* d_scratch        = nullptr;
+  uint64_t scratch_bytes = 0;
+  // end of the plan's last persistent / graph run: its pinned staging is free once it completes
+  cudaEvent_t staging_ev = nullptr;
+  bool staging_pending   = false;
 };
 
 namespace {
@@ -346,6 +352,8 @@ int mvbt_batch_plan_destroy(mvbt_batch_plan* p) {
   cudaFree(p->d_cursor);
   cudaFreeHost(p->h_batch_off);
   cudaFreeHost(p->h_params);
+  if (p->d_scratch) cudaFree(p->d_scratch);
+  if (p->staging_ev) cudaEventDestroy(p->staging_ev);
   mvbt_batch_plan_timing(p, 0);
   delete p;
   return MVBT_OK;
@@ -356,6 +364,23 @@ int mvbt_batch_plan_destroy(mvbt_batch_plan* p) {
 // mvbt_batch_run does: it owns one plan per pipeline slot and reuses a plan only after that
 // slot's previous launch has completed.
 uint64_t* mvbt_internal_plan_staging(mvbt_batch_plan* p) { return p->h_batch_off; }
+
+// Device scratch of at least `bytes` owned by the plan (mvbt_compact.cu); grows by reallocation
+// after the device is idle, so callers allocate it once, outside any timed region, by a first call.
+void* mvbt_internal_plan_scratch(mvbt_batch_plan* p, uint64_t bytes) {
+  if (!p) return nullptr;
+  if (p->scratch_bytes >= bytes) return p->d_scratch;
+  cudaDeviceSynchronize();
+  if (p->d_scratch) cudaFree(p->d_scratch);
+  p->d_scratch     = nullptr;
+  p->scratch_bytes = 0;
+  if (cudaMalloc(&p->d_scratch, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  p->scratch_bytes = bytes;
+  return p->d_scratch;
+}
 
 int mvbt_internal_batch_enqueue(mvbt_batch_plan* p, uint32_t num_batches, const uint32_t* type,
                                 const uint32_t* key, const uint32_t* arg, const uint64_t* out_off,
@@ -434,14 +459,23 @@ int mvbt_batch_run(mvbt_batch_plan* p, uint32_t num_batches, const uint64_t* bat
     return MVBT_OK;
   }
 
-  // stage the batch list in pinned memory (the captured graph copies from here)
-  MVBT_TRY(cudaStreamSynchronize(s));  // the previous run may still read the staging area
+  // stage the batch list in pinned memory (the captured graph copies from here); the plan's
+  // previous run may still read it: wait for that run alone, so a caller can queue work on other
+  // plans and streams meanwhile
+  if (p->staging_pending) MVBT_TRY(cudaEventSynchronize(p->staging_ev));
   std::memcpy(p->h_batch_off, batch_off, (num_batches + 1) * sizeof(uint64_t));
   for (uint32_t b = num_batches + 1; b <= p->max_batches; ++b) p->h_batch_off[b] = total;
   p->h_params[0] = num_batches;
   p->h_params[1] = 0;
 
-  if (mode == MVBT_BATCH_PERSISTENT) return enqueue_persistent(p, c, B, s);
+  if (!p->staging_ev) MVBT_TRY(cudaEventCreateWithFlags(&p->staging_ev, cudaEventDisableTiming));
+  if (mode == MVBT_BATCH_PERSISTENT) {
+    int rs = enqueue_persistent(p, c, B, s);
+    if (rs) return rs;
+    MVBT_TRY(cudaEventRecord(p->staging_ev, s));
+    p->staging_pending = true;
+    return MVBT_OK;
+  }
   if (p->timing) return fail(MVBT_ERR_BAD_ARG, "kernel timing is available in MVBT_BATCH_PERSISTENT mode");
   if (mode != MVBT_BATCH_GRAPH) return fail(MVBT_ERR_BAD_ARG, "unknown batch mode");
 
@@ -468,6 +502,8 @@ int mvbt_batch_run(mvbt_batch_plan* p, uint32_t num_batches, const uint64_t* bat
     std::memcpy(p->graph_key, key_now, sizeof(key_now));
   }
   MVBT_TRY(cudaGraphLaunch(p->graph, s));
+  MVBT_TRY(cudaEventRecord(p->staging_ev, s));
+  p->staging_pending = true;
   return MVBT_OK;
 }
 

@@ -78,3 +78,41 @@ def test_batches_see_every_earlier_batch_and_snapshots_advance(torch):
     er, eo = m.run_batches(b)
     assert np.array_equal(r, er) and np.array_equal(o, eo)
     assert t.take_snapshot() == m.take_snapshot() == e0 + 1 + 200
+
+
+@pytest.mark.parametrize("dest", ["device", "pinned"])
+def test_compact_range_output_packs_the_pairs_that_exist(torch, dest):
+    """mvbt_batch_compact_ranges: every range query's first min(count, cap) pairs, in op order,
+    packed contiguously (into device memory, or straight into pinned host memory)."""
+    from mvgpubtree_b200 import workload as wl
+    import mvgpubtree_b200 as mv
+    initial, seed = 100_000, 29
+    init = wl.distinct_keys(seed, 0, initial)
+    t = mv.gpu_versioned_btree(pool_bytes=1 << 28)
+    t.insert(torch.from_numpy(init.view(np.int32)).cuda(), torch.from_numpy(wl.values_for(init, 0).view(np.int32)).cuda())
+    gen = wl.MixGenerator(seed, initial, stride=wl.stride_for(initial), batch_median=4096.0,
+                          batch_min=256, batch_max=32768)
+    b = gen.generate(12)
+    d = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.int64 if a.dtype == np.uint64 else np.int32)).cuda()
+    ops = [d(b.type), d(b.key), d(b.arg), d(b.out_off), d(b.range_cap)]
+    res = torch.empty(b.num_ops, dtype=torch.int32, device="cuda")
+    rout = torch.full((b.range_pairs * 2,), -1, dtype=torch.int32, device="cuda")
+    plan = t.batch_plan(b.num_ops, 12)
+    plan.run(b.batch_off, *ops, res, rout)
+    if dest == "device":
+        comp = torch.full((b.range_pairs * 2,), -1, dtype=torch.int32, device="cuda")
+        total = torch.zeros(1, dtype=torch.int64, device="cuda")
+    else:
+        comp = torch.full((b.range_pairs * 2,), -1, dtype=torch.int32).pin_memory()
+        total = torch.zeros(1, dtype=torch.int64).pin_memory()
+    plan.compact_ranges(b.num_ops, ops[0], res, ops[3], ops[4], rout, comp, total)
+    torch.cuda.synchronize()
+    r = res.cpu().numpy().view(np.uint32)
+    ro = rout.cpu().numpy().view(np.uint32).reshape(-1, 2)
+    rq = np.nonzero(b.type == 3)[0]
+    want = np.concatenate([ro[int(b.out_off[i]): int(b.out_off[i]) + min(int(r[i]), int(b.range_cap[i]))]
+                           for i in rq]) if rq.size else np.zeros((0, 2), np.uint32)
+    got_total = int(total.cpu().numpy()[0])
+    assert got_total == len(want) and got_total > 0
+    got = comp.cpu().numpy().view(np.uint32).reshape(-1, 2)[:got_total]
+    assert np.array_equal(got, want)
