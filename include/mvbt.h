@@ -267,7 +267,7 @@ int mvbt_batch_compact_ranges(mvbt_batch_plan* plan, uint64_t num_ops, const uin
 
 /* Launch shape of the plan's persistent path (the autotuner's knobs): tile width 8 or 16 (0 = the
  * tree's; the node format is the same for both) and resident blocks per SM (-1 = the tree's,
- * 0 = full occupancy, 6 and 8 pick register-capped kernel variants). Drops a captured graph. */
+ * 0 = full occupancy, 4, 6 and 8 pick register-capped kernel variants). Drops a captured graph. */
 int mvbt_batch_plan_set_launch(mvbt_batch_plan* plan, int tile_width, int blocks_per_sm);
 
 /* Runs num_batches batches. batch_off is a HOST array of num_batches + 1 offsets; the op arrays

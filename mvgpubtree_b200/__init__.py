@@ -506,7 +506,7 @@ class BatchPlan:
 
     def set_launch(self, tile_width: int = 0, blocks_per_sm: int = -1) -> None:
         """Launch shape of the persistent path: tile width 8 / 16 (0 = the tree's) and resident
-        blocks per SM (-1 = the tree's, 0 = full occupancy, 6 / 8 = register-capped variants)."""
+        blocks per SM (-1 = the tree's, 0 = full occupancy, 4 / 6 / 8 = register-capped variants)."""
         _check(lib.mvbt_batch_plan_set_launch(self._h, int(tile_width), int(blocks_per_sm)), "set_launch")
         self.launch = (int(tile_width), int(blocks_per_sm))
 

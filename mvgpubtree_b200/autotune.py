@@ -8,13 +8,13 @@ the persistent kernel; the candidate with the least kernel time wins and is set 
 
 Knobs: tile width 8 or 16 (the node is 16 pairs, so an 8-lane tile reads it with 16-byte lane
 loads and a 16-lane tile with 8-byte loads) and blocks per SM (0 = full occupancy of the
-unconstrained kernel, 6 / 8 = register-capped variants with more resident warps).
+unconstrained kernel, 4 / 6 / 8 = register-capped variants with more resident warps).
 """
 from __future__ import annotations
 
 import numpy as np
 
-DEFAULT_CANDIDATES = ((8, 0), (8, 6), (16, 0), (16, 6))
+DEFAULT_CANDIDATES = ((8, 0), (8, 4), (8, 6), (16, 0), (16, 4), (16, 6))
 
 
 def _dev(torch, a):

@@ -98,7 +98,7 @@ def test_launch_shapes_give_identical_batch_results(torch):
                           batch_min=256, batch_max=32768)
     steps = [gen.generate(24) for _ in range(2)]
     outs = {}
-    for shape in ((8, 0), (8, 6), (8, 8), (16, 0), (16, 6), (16, 8)):
+    for shape in ((8, 0), (8, 4), (8, 6), (8, 8), (16, 0), (16, 4), (16, 6), (16, 8)):
         c = base.clone()
         p = c.batch_plan(max(b.num_ops for b in steps), 24)
         p.set_launch(*shape)
