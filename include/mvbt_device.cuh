@@ -957,10 +957,10 @@ struct device_tree {
   // ------------------------------------------------------------------------------------------
   template <int W, class Tile>
   MVBT_DEV uint32_t cooperative_find(uint32_t key, const Tile& t, uint32_t ts = kLatest,
-                                     bool concurrent = false) const {
+                                     bool concurrent = false, uint32_t start = kAnchor) const {
     const bool snap   = versioned && ts != kLatest;
     const bool seqlk  = !snap && concurrent;  // newest state under writers: read leaves locked-free
-    uint32_t idx      = kAnchor;
+    uint32_t idx      = start;  // the anchor, or a node on key's route found earlier
     bool via_older    = false;  // idx was reached through an older-version pointer
     bool leaf_next    = false;  // idx is a leaf (child of a level-1 node, or a leaf's sibling)
     node_regs<W> n;
@@ -1017,12 +1017,13 @@ struct device_tree {
   // ------------------------------------------------------------------------------------------
   template <int W, class Tile>
   MVBT_DEV uint32_t cooperative_range_query(uint32_t lo, uint32_t hi, const Tile& t, uint32_t ts,
-                                            uint2* out, uint32_t cap, bool concurrent = false) const {
+                                            uint2* out, uint32_t cap, bool concurrent = false,
+                                            uint32_t start = kAnchor) const {
     constexpr int P = 16 / W;
     if (hi <= lo) return 0;
     const bool snap  = versioned && ts != kLatest;
     const bool seqlk = !snap && concurrent;  // newest state under writers (read_leaf_latest)
-    uint32_t idx     = kAnchor;
+    uint32_t idx     = start;  // the anchor, or a node on lo's route found earlier
     bool via_older   = false;
     bool leaf_next   = false;
     node_regs<W> n;
@@ -1344,10 +1345,20 @@ struct device_tree {
   template <int W, class Tile>
   MVBT_DEV bool cooperative_insert(uint32_t key, uint32_t value, const Tile& t, uint32_t E) const {
     if (key == kEmptyKey) return false;
+    uint32_t path0 = kNone, path1 = kNone, top = 0;
+    const uint32_t leaf = descend_for_write<W>(key, path0, path1, top, t);
+    if (leaf == kNone) return false;
+    return insert_at<W>(key, value, t, E, leaf, path0, path1, top);
+  }
+
+  // The insert after its descent: `leaf` and the path (path0 / path1 / top, as descend_for_write
+  // records them) may have been found before other writers changed the tree; lock_covering moves
+  // right as far as needed and a stale path entry only lengthens the approach to a parent.
+  template <int W, class Tile>
+  MVBT_DEV bool insert_at(uint32_t key, uint32_t value, const Tile& t, uint32_t E, uint32_t leaf,
+                          uint32_t path0, uint32_t path1, uint32_t top) const {
+    if (key == kEmptyKey) return false;
     {
-      uint32_t path0 = kNone, path1 = kNone, top = 0;
-      uint32_t leaf = descend_for_write<W>(key, path0, path1, top, t);
-      if (leaf == kNone) return false;
       node_regs<W> n;
       header h;
       leaf = lock_covering<W>(leaf, 0, key, n, h, t);
@@ -1424,8 +1435,15 @@ struct device_tree {
   MVBT_DEV bool cooperative_erase(uint32_t key, const Tile& t, uint32_t E) const {
     if (key == kEmptyKey) return false;
     uint32_t path0 = kNone, path1 = kNone, top = 0;
-    uint32_t leaf = descend_for_write<W>(key, path0, path1, top, t);
+    const uint32_t leaf = descend_for_write<W>(key, path0, path1, top, t);
     if (leaf == kNone) return false;
+    return erase_at<W>(key, t, E, leaf);
+  }
+
+  // The erase after its descent (the leaf may be stale: lock_covering moves right).
+  template <int W, class Tile>
+  MVBT_DEV bool erase_at(uint32_t key, const Tile& t, uint32_t E, uint32_t leaf) const {
+    if (key == kEmptyKey) return false;
     node_regs<W> n;
     header h;
     leaf = lock_covering<W>(leaf, 0, key, n, h, t);
@@ -1497,6 +1515,43 @@ MVBT_DEV bool run_batch_op(const device_tree& T, const batch_view& B, uint64_t i
     write = true;
   } else if (ty == kOpErase) {
     T.cooperative_erase<W>(k, t, E);
+    write = true;
+  }
+  if (t.thread_rank() == 0) B.result[i] = r;
+  return write;
+}
+
+// An op whose batch is not ready yet does its descent first (routing at the newest state; nothing
+// it returns depends on the batches still running), then waits, then finishes from the leaf it
+// found: run_batch_op_at. Readers start their snapshot read at that leaf -- its low fence is fixed
+// for life, a node made after the snapshot leads to the version the snapshot reads through its
+// older pointer, and the fence checks move right or restart as needed -- and writers lock the
+// covering leaf from it. Returns the leaf (kNone: fall back to the whole op).
+template <int W, class Tile>
+MVBT_DEV uint32_t batch_op_descend(const device_tree& T, const batch_view& B, uint64_t i, uint32_t& path0,
+                                   uint32_t& path1, uint32_t& top, const Tile& t) {
+  const uint32_t k = B.key[i];
+  if (k == kEmptyKey) return kNone;
+  return T.descend_for_write<W>(k, path0, path1, top, t);
+}
+
+template <int W, class Tile>
+MVBT_DEV bool run_batch_op_at(const device_tree& T, const batch_view& B, uint64_t i, uint32_t S, uint32_t E,
+                              const Tile& t, uint32_t leaf, uint32_t path0, uint32_t path1, uint32_t top) {
+  if (leaf == kNone) return run_batch_op<W>(T, B, i, S, E, t);
+  const uint32_t ty = B.type[i], k = B.key[i];
+  uint32_t r        = 0;
+  bool write        = false;
+  if (ty == kOpFind) {
+    r = T.cooperative_find<W>(k, t, S, true, leaf);
+  } else if (ty == kOpRange) {
+    uint2* out = B.range_out ? B.range_out + B.out_off[i] : nullptr;
+    r          = T.cooperative_range_query<W>(k, B.arg[i], t, S, out, B.cap[i], true, leaf);
+  } else if (ty == kOpInsert) {
+    T.insert_at<W>(k, B.arg[i], t, E, leaf, path0, path1, top);
+    write = true;
+  } else if (ty == kOpErase) {
+    T.erase_at<W>(k, t, E, leaf);
     write = true;
   }
   if (t.thread_rank() == 0) B.result[i] = r;
@@ -1603,10 +1658,11 @@ MVBT_DEV void batched_worker(const device_tree& T, const batch_view& B, const ba
     __threadfence();  // the batches counted in d are finished: see their writes
     warp.sync();
     bool did = false;
-    // writes first: they gate every later batch
+    // writes first: they gate every later batch. Work is taken up to one batch past the finished
+    // ones; an op of a batch that is not ready does its descent, then waits (run_batch_op_at).
     if (g < TW) {
       wb = batch_of_ordinal(sc.wpre, nb, g, wb);
-      if (wb <= d) {
+      if (wb <= d + 1) {
         unsigned long long g0 = 0;
         if (warp.thread_rank() == 0) g0 = atomicAdd(sc.wcursor, (unsigned long long)(kTiles * kWriteClaim));
         g0 = warp.shfl(g0, 0);
@@ -1616,12 +1672,16 @@ MVBT_DEV void batched_worker(const device_tree& T, const batch_view& B, const ba
           const unsigned long long x = g0 + k * kTiles + tid;
           if (x >= TW) break;
           b = batch_of_ordinal(sc.wpre, nb, x, b);
+          const uint32_t i = sc.perm[sc.batch_off[b] + (x - sc.wpre[b])];
           if (b > dd) {
+            uint32_t p0 = kNone, p1 = kNone, top = 0;
+            const uint32_t leaf = batch_op_descend<W>(T, B, i, p0, p1, top, t);
             if (!wait_batch_ready(T, sc, nb, b, t) && t.thread_rank() == 0) T.set_error(kErrSpinLimit, 14);
             dd = b;
+            run_batch_op_at<W>(T, B, i, S0 + b, S0 + b + 1, t, leaf, p0, p1, top);
+          } else {
+            run_batch_op<W>(T, B, i, S0 + b, S0 + b + 1, t);
           }
-          const uint32_t i = sc.perm[sc.batch_off[b] + (x - sc.wpre[b])];
-          run_batch_op<W>(T, B, i, S0 + b, S0 + b + 1, t);
           __threadfence();
           t.sync();
           if (t.thread_rank() == 0) {
@@ -1633,7 +1693,7 @@ MVBT_DEV void batched_worker(const device_tree& T, const batch_view& B, const ba
     }
     if (!did && r < TR) {
       rb = batch_of_ordinal(sc.rpre, nb, r, rb);
-      if (rb <= d) {
+      if (rb <= d + 1) {
         unsigned long long r0 = 0;
         if (warp.thread_rank() == 0) r0 = atomicAdd(sc.rcursor, (unsigned long long)(kTiles * kReadClaim));
         r0 = warp.shfl(r0, 0);
@@ -1643,12 +1703,16 @@ MVBT_DEV void batched_worker(const device_tree& T, const batch_view& B, const ba
           const unsigned long long x = r0 + k * kTiles + tid;
           if (x >= TR) break;
           b = batch_of_ordinal(sc.rpre, nb, x, b);
+          const uint32_t i = sc.perm[sc.batch_off[b] + sc.n_writes[b] + (x - sc.rpre[b])];
           if (b > dd) {
+            uint32_t p0 = kNone, p1 = kNone, top = 0;
+            const uint32_t leaf = batch_op_descend<W>(T, B, i, p0, p1, top, t);
             if (!wait_batch_ready(T, sc, nb, b, t) && t.thread_rank() == 0) T.set_error(kErrSpinLimit, 14);
             dd = b;
+            run_batch_op_at<W>(T, B, i, S0 + b, S0 + b + 1, t, leaf, p0, p1, top);
+          } else {
+            run_batch_op<W>(T, B, i, S0 + b, S0 + b + 1, t);
           }
-          const uint32_t i = sc.perm[sc.batch_off[b] + sc.n_writes[b] + (x - sc.rpre[b])];
-          run_batch_op<W>(T, B, i, S0 + b, S0 + b + 1, t);
         }
       }
     }

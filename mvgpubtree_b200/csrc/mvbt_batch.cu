@@ -227,7 +227,7 @@ void launch_batched(const launch_ctx& c, const batch_view& B, const batch_sched&
   if (c.bps >= 8) k_batched<W, 8><<<occupancy_grid(c, k_batched<W, 8>), c.block, 0, s>>>(c.view, B, sc);
   else if (c.bps >= 6) k_batched<W, 6><<<occupancy_grid(c, k_batched<W, 6>), c.block, 0, s>>>(c.view, B, sc);
   else if (c.bps >= 4) k_batched<W, 4><<<occupancy_grid(c, k_batched<W, 4>), c.block, 0, s>>>(c.view, B, sc);
-  else k_batched<W, 1><<<occupancy_grid(c, k_batched<W, 1>), c.block, 0, s>>>(c.view, B, sc);
+  else k_batched<W, 3><<<occupancy_grid(c, k_batched<W, 3>), c.block, 0, s>>>(c.view, B, sc);
 }
 
 // One batch [begin, end) in one launch: reads at the snapshot in snap_word, writes one epoch later.
