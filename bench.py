@@ -19,6 +19,9 @@ serving  : continuous batching of Poisson-arriving requests (lognormal sizes, me
            offered loads of 10 / 50 / 200 M ops/s for a short window each, on a 40M-key tree with
            reclamation; p50 / p99 / p999 latency (arrival to results on the host) and achieved
            throughput, beside the plain mode with one request per launch on an identical tree.
+configs  : the other workloads of the reference's benchmarks, measured alone before the above:
+           c1 plain-tree insert + finds (2^20 keys), c2 versioned insert / update / finds at two
+           snapshots (2^25 keys), c3 concurrent insert + range on 40M keys (9 mixes).
 
 With --impl reference the script times the reference implementation's own CUDA build
 (oracle/_ref/ref_driver, built by oracle/ref_build.py from the reference's unmodified headers) on
@@ -75,6 +78,11 @@ def parse_args():
                     help="offered loads (M ops/s) of the serving sessions; empty = no serving run")
     ap.add_argument("--serve-seconds", type=float, default=0.25,
                     help="arrival window of each serving session")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the c1-c3 workloads (plain finds, finds at snapshots, concurrent "
+                         "insert + range) reported under \"configs\"")
+    ap.add_argument("--config-reps", type=int, default=2,
+                    help="timed experiments per c1-c3 measurement (after one untimed)")
     return ap.parse_args()
 
 
@@ -528,6 +536,196 @@ def cpu_oracle_time(init, vals, batches, max_ops: int):
 
 REF_DRIVER = Path(__file__).resolve().parent / "oracle" / "_ref" / "ref_driver"
 
+# ------------------------------------------------------------------------------------------------
+# the other workloads of the reference's own benchmarks, in both arms (configs 1-3)
+#   c1: plain B-link tree, 2^20 keys inserted, 2^20 finds (half hits)
+#   c2: versioned tree, 2^25 keys, 2^22 in-place updates, 2^25 finds at the snapshot before and
+#       at the snapshot after the updates
+#   c3: versioned tree of 40M keys, 10M ops in one concurrent_insert_range call (each op an insert
+#       with probability u, else a range query of length L), u in {5, 50, 90} %, L in {8, 32, 128}
+# Every phase is timed alone with CUDA events, after one untimed experiment, mean of --config-reps.
+# ------------------------------------------------------------------------------------------------
+C1_KEYS, C2_KEYS, C2_UPDATES = 1 << 20, 1 << 25, 1 << 22
+C3_OPS, C3_UPDATE, C3_LENGTHS = 10_000_000, (0.05, 0.5, 0.9), (8, 32, 128)
+
+
+def hit_miss_queries(wl, seed: int, keys: np.ndarray) -> np.ndarray:
+    n = keys.size
+    hits = wl.shuffle(seed + 1, keys)[: n // 2]
+    miss = wl.distinct_keys(seed, wl.MISS_INDEX_BASE, n - n // 2)
+    return wl.shuffle(seed + 2, np.concatenate([hits, miss]))
+
+
+def c3_combos(seed: int):
+    """(u, L, inserts, ranges) of config 3: each of the 10M ops is an insert with probability u."""
+    out = []
+    for u in C3_UPDATE:
+        n_ins = int((np.random.default_rng(seed).random(C3_OPS) < u).sum())
+        out += [(u, L, n_ins, C3_OPS - n_ins) for L in C3_LENGTHS]
+    return out
+
+
+def _hmean(xs):
+    return len(xs) / sum(1.0 / x for x in xs)
+
+
+def run_configs_ours(args) -> dict:
+    """Configs 1-3 through this library's reference-named host API, tile widths 8 and 16 (the
+    faster is reported). Results are checked where a full-size check is cheap: every c1 and c2 find
+    against the value function of its key."""
+    import torch
+    import mvgpubtree_b200 as mv
+    from mvgpubtree_b200 import workload as wl
+
+    seed, reps = args.seed, max(1, args.config_reps)
+    stream = torch.cuda.current_stream()
+
+    def dev(a):
+        return torch.from_numpy(np.ascontiguousarray(a).view(np.int32)).cuda()
+
+    def timed(fn):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        fn()
+        b.record(stream)
+        b.synchronize()
+        return a.elapsed_time(b)
+
+    def mean_runs(make, phases):
+        """1 untimed + reps timed experiments of make() -> tree, then phases(tree) -> [ms...]."""
+        acc = None
+        for r in range(1 + reps):
+            t = make()
+            ms = phases(t)
+            t.check_errors()
+            t.close()
+            if r:
+                acc = ms if acc is None else [x + y for x, y in zip(acc, ms)]
+        return [x / reps for x in acc]
+
+    out = {}
+    # ---- c1 ----
+    n = C1_KEYS
+    keys = wl.distinct_keys(seed, 0, n)
+    vals = wl.values_for(keys, seed)
+    q = hit_miss_queries(wl, seed, keys)
+    expect = np.where(np.isin(q, keys, assume_unique=True), wl.values_for(q, seed), 0xFFFFFFFF).astype(np.uint32)
+    dk, dv, dq = dev(keys), dev(vals), dev(q)
+    r0 = torch.empty(n, dtype=torch.int32, device="cuda")
+    best = None
+    for w in (8, 16):
+        ms = mean_runs(lambda: mv.gpu_blink_tree(pool_bytes=1 << 30, tile_width=w),
+                       lambda t: [timed(lambda: t.insert(dk, dv)), timed(lambda: t.find(dq, r0))])
+        ok = bool(np.array_equal(r0.cpu().numpy().view(np.uint32), expect))
+        row = {"tile_width": w, "insert_mops": round(n / ms[0] / 1e3, 1), "find_mops": round(n / ms[1] / 1e3, 1),
+               "verified": ok}
+        if best is None or row["find_mops"] > best["find_mops"]:
+            best = row
+    out["c1_plain_2^20"] = best
+    del dk, dv, dq, r0
+
+    # ---- c2 ----
+    n, u = C2_KEYS, C2_UPDATES
+    keys = wl.distinct_keys(seed, 0, n)
+    upd = wl.shuffle(seed + 3, keys)[:u]
+    q = hit_miss_queries(wl, seed, keys)
+    hit = np.isin(q, keys, assume_unique=True)
+    e0 = np.where(hit, wl.values_for(q, seed), 0xFFFFFFFF).astype(np.uint32)
+    e1 = np.where(np.isin(q, upd, assume_unique=True), wl.values_for(q, seed ^ 1), e0).astype(np.uint32)
+    dk, dv, du, duv, dq = dev(keys), dev(wl.values_for(keys, seed)), dev(upd), dev(wl.values_for(upd, seed ^ 1)), dev(q)
+    r0 = torch.empty(n, dtype=torch.int32, device="cuda")
+    r1 = torch.empty(n, dtype=torch.int32, device="cuda")
+    best = None
+    for w in (8, 16):
+        def phases(t):
+            a = timed(lambda: t.insert(dk, dv))
+            s0 = t.take_snapshot()
+            b = timed(lambda: t.insert(du, duv))
+            s1 = t.take_snapshot()
+            return [a, b, timed(lambda: t.find(dq, r0, timestamp=s0)), timed(lambda: t.find(dq, r1, timestamp=s1))]
+        ms = mean_runs(lambda: mv.gpu_versioned_btree(pool_bytes=4 << 30, tile_width=w), phases)
+        ok = bool(np.array_equal(r0.cpu().numpy().view(np.uint32), e0)
+                  and np.array_equal(r1.cpu().numpy().view(np.uint32), e1))
+        row = {"tile_width": w, "insert_mops": round(n / ms[0] / 1e3, 1), "update_mops": round(u / ms[1] / 1e3, 1),
+               "find_s0_mops": round(n / ms[2] / 1e3, 1), "find_s1_mops": round(n / ms[3] / 1e3, 1),
+               "verified": ok}
+        if best is None or row["find_s1_mops"] > best["find_s1_mops"]:
+            best = row
+    out["c2_versioned_2^25"] = best
+    del dk, dv, du, duv, dq, r0, r1
+    torch.cuda.empty_cache()
+
+    # ---- c3: concurrent insert + range query on clones of one 40M-key tree per tile width ----
+    N = args.initial_keys
+    stride = wl.stride_for(N)
+    keys = wl.distinct_keys(seed, 0, N)
+    dk, dv = dev(keys), dev(wl.values_for(keys, seed))
+    base, insert_mops = {}, {}
+    for w in (8, 16):
+        ms = []
+        for r in range(1 + reps):
+            t = mv.gpu_versioned_btree(pool_bytes=8 << 30, tile_width=w)
+            ms.append(timed(lambda: t.insert(dk, dv)))
+            if r < reps:
+                t.close()
+        base[w] = t
+        insert_mops[w] = round(N / (sum(ms[1:]) / reps) / 1e3, 1)
+    del dk, dv
+    runs = {8: {}, 16: {}}
+    for u, L, n_ins, n_rq in c3_combos(seed):
+        ins = wl.distinct_keys(seed, N, n_ins)
+        lo = wl.uniform_keys(seed + 1, n_rq)
+        di, div, dlo, dhi = dev(ins), dev(wl.values_for(ins, seed)), dev(lo), dev(wl.upper_bounds(lo, L, stride))
+        pairs = torch.empty(n_rq * 2 * L * 2, dtype=torch.int32, device="cuda")
+        for w in (8, 16):
+            ms = mean_runs(lambda: base[w].clone(),
+                           lambda t: [timed(lambda: t.concurrent_insert_range(
+                               di, div, n_ins, dlo, dhi, n_rq, pairs, 2 * L))])
+            runs[w][f"u{int(u * 100)}_L{L}"] = round(C3_OPS / ms[0] / 1e3, 1)
+        del di, div, dlo, dhi, pairs
+        torch.cuda.empty_cache()
+    for t in base.values():
+        t.close()
+    w = max(runs, key=lambda k: _hmean(list(runs[k].values())))
+    out["c3_concurrent_insert_range_40M"] = {
+        "tile_width": w, "insert_40M_mops": insert_mops[w], "ops_mops": runs[w],
+        "ops_hmean_mops": round(_hmean(list(runs[w].values())), 1)}
+    torch.cuda.empty_cache()
+    return out
+
+
+def run_configs_reference(args) -> dict:
+    """Configs 1-3 on the reference implementation's own CUDA build (oracle/_ref/ref_driver): the
+    same inputs and phases as run_configs_ours, through the reference's public host API."""
+    if not REF_DRIVER.exists():
+        return {"unavailable": "reference build not present"}
+    reps = str(max(1, args.config_reps))
+    common = ["--seed", str(args.seed), "--warmup", "1", "--reps", reps]
+
+    def drive(*a):
+        out = subprocess.run([str(REF_DRIVER), *a, *common], capture_output=True, text=True, timeout=1200)
+        if out.returncode != 0:
+            raise RuntimeError(f"ref_driver {a[0]} failed ({out.returncode}): {out.stderr.strip()[-300:]}")
+        return json.loads(out.stdout.strip().splitlines()[-1])
+
+    res = {}
+    try:
+        c1 = drive("c1", "--n", str(C1_KEYS))
+        res["c1_plain_2^20"] = {"insert_mops": round(c1["insert_mops"], 1), "find_mops": round(c1["find_mops"], 1)}
+        c2 = drive("c2", "--initial", str(C2_KEYS), "--updates", str(C2_UPDATES))
+        res["c2_versioned_2^25"] = {"insert_mops": round(c2["insert_mops"], 1), "update_mops": round(c2["update_mops"], 1),
+                                    "find_s0_mops": round(c2["find0_mops"], 1), "find_s1_mops": round(c2["find1_mops"], 1)}
+        combos = c3_combos(args.seed)
+        spec = ",".join(f"{i}:{r}:{L}:{2 * L}" for _, L, i, r in combos)
+        c3 = drive("c3", "--initial", str(args.initial_keys), "--combos", spec, "--checksums", "0")
+        ops = {f"u{int(u * 100)}_L{L}": round(x["ops_mops"], 1) for (u, L, _, _), x in zip(combos, c3["runs"])}
+        res["c3_concurrent_insert_range_40M"] = {
+            "insert_40M_mops": round(statistics.mean(x["insert_mops"] for x in c3["runs"]), 1),
+            "ops_mops": ops, "ops_hmean_mops": round(_hmean(list(ops.values())), 1)}
+    except (RuntimeError, subprocess.TimeoutExpired) as e:
+        res["error"] = str(e)[-300:]
+    return res
+
 
 def reference_build_time(args, W: int, K: int):
     """The reference implementation's own CUDA build (oracle/_ref/ref_driver, compiled from the
@@ -554,6 +752,7 @@ def run_reference(args, dist: Dist):
     if dist.rank != 0:
         return None
     W, K = max(3, args.warmup), args.steps
+    configs = None if args.no_configs else run_configs_reference(args)
     ref, why = reference_build_time(args, W, K)
     init, vals, steps, _ = make_workload(args.seed, args.initial_keys, W + K, args.batches)
     cores, build_s, times, ops = cpu_oracle_time(init, vals, steps, args.cpu_sample_ops)
@@ -583,6 +782,7 @@ def run_reference(args, dist: Dist):
         "data": "synthetic (seeded)", "config": config,
         "cpu_baseline": cpu,
         "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        **({"configs": configs} if configs is not None else {}),
     }
 
 
@@ -594,7 +794,12 @@ def main():
         if out is not None:
             print(json.dumps(out), flush=True)
         return
+    configs = None
+    if dist.world == 1 and not args.no_configs:
+        configs = run_configs_ours(args)
     out, cpu_inputs = run_ours(args, dist)
+    if configs is not None:
+        out["configs"] = configs
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
         init, vals, step = cpu_inputs
         cores, build_s, times, ops = cpu_oracle_time(init, vals, [step], args.cpu_sample_ops)

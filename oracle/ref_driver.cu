@@ -5,11 +5,19 @@
 // the tests and bench.py's reference arm run it.
 //
 // Modes:
-//   c1 --n N --seed S
+//   c1 --n N --seed S [--warmup W] [--reps R]
 //      Plain B-link tree, GpuBTree::gpu_blink_tree<uint32_t, uint32_t> (reference
 //      include/gpu_blink_tree.hpp:63-67): insert N distinct keys of seed S with values
 //      fmix32(key ^ S), then N finds shuffled from N/2 inserted keys and N - N/2 keys that were
 //      never inserted (include/gpu_blink_tree.hpp:218-236).
+//   c2 --initial N --updates U --seed S [--warmup W] [--reps R]
+//      Versioned tree: insert, snapshot S0, update U keys in place, snapshot S1, the queries of c1
+//      at S0 and at S1; each phase timed alone (run_c2).
+//   c3 --initial N --seed S [--stride D] --combos I:R:L:Q[,...] [--warmup W] [--reps R]
+//      [--checksums 0|1] [--dump PREFIX]
+//      Versioned tree: the reference's concurrent_insert_range timed per combination on a fresh
+//      tree, and a deterministic insert / snapshot / insert / range_query sequence checked
+//      (run_c3).
 //   c4 --initial N --batches B --steps K --warmup W --seed S [--stride D] [--median M]
 //      [--batch-min A] [--batch-max Z] [--final-chunks C] [--checksums 0|1]
 //      Versioned tree, GpuBTree::gpu_versioned_btree<uint32_t, uint32_t>
@@ -79,17 +87,18 @@ uint64_t pair_term(uint64_t i, uint64_t j, uint32_t k, uint32_t v) {
 
 struct args_t {
   std::string mode;
-  uint64_t n = 1 << 20, initial = 1 << 20, seed = 1;
-  uint32_t batches = 16, steps = 1, warmup = 0, final_chunks = 0, checksums = 1;
+  uint64_t n = 1 << 20, initial = 1 << 20, seed = 1, updates = 0;
+  uint32_t batches = 16, steps = 1, warmup = 0, final_chunks = 0, checksums = 1, reps = 1;
   uint64_t stride = 0;
   double median = 0;
   uint32_t batch_min = 0, batch_max = 0;
+  std::string combos, dump;
 };
 
 args_t parse(int argc, char** argv) {
   args_t a;
   if (argc < 2) {
-    std::fprintf(stderr, "usage: ref_driver c1|c4 [--key value]...\n");
+    std::fprintf(stderr, "usage: ref_driver c1|c2|c3|c4 [--key value]...\n");
     std::exit(2);
   }
   a.mode = argv[1];
@@ -108,6 +117,10 @@ args_t parse(int argc, char** argv) {
     else if (k == "--median") a.median = std::strtod(v, nullptr);
     else if (k == "--batch-min") a.batch_min = (uint32_t)std::strtoul(v, nullptr, 10);
     else if (k == "--batch-max") a.batch_max = (uint32_t)std::strtoul(v, nullptr, 10);
+    else if (k == "--updates") a.updates = std::strtoull(v, nullptr, 10);
+    else if (k == "--reps") a.reps = (uint32_t)std::strtoul(v, nullptr, 10);
+    else if (k == "--combos") a.combos = v;
+    else if (k == "--dump") a.dump = v;
     else {
       std::fprintf(stderr, "ref_driver: unknown option %s\n", k.c_str());
       std::exit(2);
@@ -141,45 +154,281 @@ float elapsed_ms(cudaEvent_t a, cudaEvent_t b) {
   return ms;
 }
 
+// Point queries of configs 1 and 2: n/2 inserted keys (a shuffle of seed + 1) and n - n/2 keys
+// that were never inserted, shuffled together with seed + 2.
+std::vector<uint32_t> hit_miss_queries(uint64_t seed, const std::vector<uint32_t>& keys) {
+  const uint64_t n = keys.size(), nh = n / 2;
+  std::vector<uint32_t> hits(keys), q(n);
+  mvbt_wl_shuffle(seed + 1, hits.data(), n);
+  std::copy(hits.begin(), hits.begin() + nh, q.begin());
+  mvbt_wl_distinct_keys(seed, MVBT_MISS_INDEX_BASE, n - nh, q.data() + nh);
+  mvbt_wl_shuffle(seed + 2, q.data(), n);
+  return q;
+}
+
+uint64_t find_checksum(const uint32_t* d, uint64_t n) {
+  auto out   = host_copy(d, n);
+  uint64_t s = 0;
+  for (uint64_t i = 0; i < n; ++i) s += find_term(i, out[i]);
+  return s;
+}
+
 int run_c1(const args_t& a) {
   const uint64_t n = a.n;
-  std::vector<uint32_t> keys(n), vals(n), q(n), out(n);
+  std::vector<uint32_t> keys(n), vals(n);
   mvbt_wl_distinct_keys(a.seed, 0, n, keys.data());
   mvbt_wl_values(keys.data(), n, (uint32_t)a.seed, vals.data());
-  std::vector<uint32_t> hits(keys);
-  mvbt_wl_shuffle(a.seed + 1, hits.data(), n);
-  const uint64_t nh = n / 2;
-  std::copy(hits.begin(), hits.begin() + nh, q.begin());
-  mvbt_wl_distinct_keys(a.seed, MVBT_MISS_INDEX_BASE, n - nh, q.data() + nh);
-  mvbt_wl_shuffle(a.seed + 2, q.data(), n);
+  std::vector<uint32_t> q = hit_miss_queries(a.seed, keys);
 
   uint32_t *dk = dev_copy(keys), *dv = dev_copy(vals), *dq = dev_copy(q), *dr = dev_alloc<uint32_t>(n);
-  btree_t tree;
   cudaEvent_t e0, e1, e2;
   check(cudaEventCreate(&e0), "event");
   check(cudaEventCreate(&e1), "event");
   check(cudaEventCreate(&e2), "event");
-  check(cudaDeviceSynchronize(), "setup");
-  check(cudaEventRecord(e0, 0), "record");
-  tree.insert(dk, dv, (uint32_t)n, 0);
-  check(cudaEventRecord(e1, 0), "record");
-  tree.find(dq, dr, (uint32_t)n, 0, false);
-  check(cudaEventRecord(e2, 0), "record");
-  check(cudaEventSynchronize(e2), "sync");
-  check(cudaGetLastError(), "kernels");
-  const float ins_ms = elapsed_ms(e0, e1), find_ms = elapsed_ms(e1, e2);
-  out = host_copy(dr, n);
-  uint64_t cs = 0;
-  for (uint64_t i = 0; i < n; ++i) cs += find_term(i, out[i]);
+  const uint32_t reps = std::max(1u, a.reps);
+  double ins_ms = 0, find_ms = 0;
+  for (uint32_t r = 0; r < a.warmup + reps; ++r) {  // fresh tree per experiment
+    btree_t tree;
+    check(cudaDeviceSynchronize(), "setup");
+    check(cudaEventRecord(e0, 0), "record");
+    tree.insert(dk, dv, (uint32_t)n, 0);
+    check(cudaEventRecord(e1, 0), "record");
+    tree.find(dq, dr, (uint32_t)n, 0, false);
+    check(cudaEventRecord(e2, 0), "record");
+    check(cudaEventSynchronize(e2), "sync");
+    check(cudaGetLastError(), "kernels");
+    if (r >= a.warmup) {
+      ins_ms += elapsed_ms(e0, e1) / reps;
+      find_ms += elapsed_ms(e1, e2) / reps;
+    }
+  }
+  const uint64_t cs = find_checksum(dr, n);
   std::printf(
-      "{\"mode\": \"c1\", \"n\": %llu, \"seed\": %llu, \"insert_ms\": %.4f, \"find_ms\": %.4f, "
+      "{\"mode\": \"c1\", \"n\": %llu, \"seed\": %llu, \"reps\": %u, \"insert_ms\": %.4f, \"find_ms\": %.4f, "
       "\"insert_mops\": %.3f, \"find_mops\": %.3f, \"find_checksum\": %llu}\n",
-      (unsigned long long)n, (unsigned long long)a.seed, ins_ms, find_ms, n / (ins_ms * 1e3), n / (find_ms * 1e3),
-      (unsigned long long)cs);
+      (unsigned long long)n, (unsigned long long)a.seed, reps, ins_ms, find_ms, n / (ins_ms * 1e3),
+      n / (find_ms * 1e3), (unsigned long long)cs);
   cudaFree(dk);
   cudaFree(dv);
   cudaFree(dq);
   cudaFree(dr);
+  return 0;
+}
+
+// Config 2: versioned tree, N keys of seed S (values fmix32(key ^ S)), snapshot S0, U of them
+// updated (a shuffle of seed S + 3, values fmix32(key ^ S ^ 1)), snapshot S1, then the N queries
+// of hit_miss_queries at S0 and at S1. Writes in place (the reference's ViB form,
+// include/gpu_versioned_blink_tree.hpp:106-142). Each phase is timed alone; the experiment runs
+// W untimed and R timed times on fresh trees and the timed phases are averaged.
+int run_c2(const args_t& a) {
+  const uint64_t n = a.initial, u = a.updates ? std::min(a.updates, n) : n / 8;
+  std::vector<uint32_t> keys(n), vals(n), upd, uvals(u);
+  mvbt_wl_distinct_keys(a.seed, 0, n, keys.data());
+  mvbt_wl_values(keys.data(), n, (uint32_t)a.seed, vals.data());
+  upd = keys;
+  mvbt_wl_shuffle(a.seed + 3, upd.data(), n);
+  upd.resize(u);
+  mvbt_wl_values(upd.data(), u, (uint32_t)a.seed ^ 1u, uvals.data());
+  std::vector<uint32_t> q = hit_miss_queries(a.seed, keys);
+  uint32_t *dk = dev_copy(keys), *dv = dev_copy(vals), *du = dev_copy(upd), *duv = dev_copy(uvals);
+  uint32_t *dq = dev_copy(q), *dr0 = dev_alloc<uint32_t>(n), *dr1 = dev_alloc<uint32_t>(n);
+  cudaEvent_t ev[7];
+  for (auto& e : ev) check(cudaEventCreate(&e), "event");
+  double ms[4] = {0, 0, 0, 0};
+  uint64_t cs0 = 0, cs1 = 0;
+  const uint32_t reps = std::max(1u, a.reps);
+  for (uint32_t r = 0; r < a.warmup + reps; ++r) {  // fresh tree per experiment
+    vtree_t tree;
+    check(cudaDeviceSynchronize(), "setup");
+    check(cudaEventRecord(ev[0], 0), "record");
+    tree.insert(dk, dv, (uint32_t)n, 0, true);
+    check(cudaEventRecord(ev[1], 0), "record");
+    const uint32_t S0 = tree.take_snapshot();  // a blocking copy, outside the timed phases
+    check(cudaEventRecord(ev[2], 0), "record");
+    tree.insert(du, duv, (uint32_t)u, 0, true);
+    check(cudaEventRecord(ev[3], 0), "record");
+    const uint32_t S1 = tree.take_snapshot();
+    check(cudaEventRecord(ev[4], 0), "record");
+    tree.find(dq, dr0, (uint32_t)n, S0, 0, false);
+    check(cudaEventRecord(ev[5], 0), "record");
+    tree.find(dq, dr1, (uint32_t)n, S1, 0, false);
+    check(cudaEventRecord(ev[6], 0), "record");
+    check(cudaEventSynchronize(ev[6]), "sync");
+    check(cudaGetLastError(), "kernels");
+    if (r < a.warmup) continue;
+    ms[0] += elapsed_ms(ev[0], ev[1]);
+    ms[1] += elapsed_ms(ev[2], ev[3]);
+    ms[2] += elapsed_ms(ev[4], ev[5]);
+    ms[3] += elapsed_ms(ev[5], ev[6]);
+    if (r + 1 == a.warmup + reps) {
+      cs0 = find_checksum(dr0, n);
+      cs1 = find_checksum(dr1, n);
+    }
+  }
+  for (double& m : ms) m /= reps;
+  std::printf(
+      "{\"mode\": \"c2\", \"initial\": %llu, \"updates\": %llu, \"seed\": %llu, \"reps\": %u, "
+      "\"insert_ms\": %.4f, \"update_ms\": %.4f, \"find0_ms\": %.4f, \"find1_ms\": %.4f, "
+      "\"insert_mops\": %.3f, \"update_mops\": %.3f, \"find0_mops\": %.3f, \"find1_mops\": %.3f, "
+      "\"find_checksums\": [%llu, %llu]}\n",
+      (unsigned long long)n, (unsigned long long)u, (unsigned long long)a.seed, reps, ms[0], ms[1], ms[2], ms[3],
+      n / (ms[0] * 1e3), u / (ms[1] * 1e3), n / (ms[2] * 1e3), n / (ms[3] * 1e3), (unsigned long long)cs0,
+      (unsigned long long)cs1);
+  for (auto& e : ev) cudaEventDestroy(e);
+  for (uint32_t* p : {dk, dv, du, duv, dq, dr0, dr1}) cudaFree(p);
+  return 0;
+}
+
+// Config 3: versioned tree of N keys of seed S (values fmix32(key ^ S)); per combination I:R:L:Q,
+// I new keys (distinct_keys(S, N, I), values fmix32(key ^ S)) and R range queries with uniform
+// lower bounds (seed S + 1) and upper = lower + L * stride, Q pairs of output per query.
+//   timed: the reference's concurrent_insert_range on a fresh tree
+//          (include/gpu_versioned_blink_tree.hpp:252-294), one kernel of inserts and queries; each
+//          query tile takes its own snapshot as it starts, so its results are not deterministic.
+//   checked (--checksums 1): insert, S0 = take_snapshot, insert of the new keys, S1 =
+//          take_snapshot, range_query at S0 and at S1 with 4L + 64 pairs per query; counts and
+//          pairs checksums, once with the second insert in place ("checksums") and once out of
+//          place ("checksums_out_of_place"); --dump P writes each count array to P_<form>_s<v>.u32.
+// The reference writes every hit of a query with no bound; each pair buffer carries a tail of
+// L * stride pairs, more than the last query's range [lo, lo + L * stride) can hold.
+struct c3_combo {
+  uint64_t inserts, ranges, length, slot;
+};
+
+std::vector<c3_combo> parse_combos(const std::string& s) {
+  std::vector<c3_combo> out;
+  size_t p = 0;
+  while (p < s.size()) {
+    size_t e = s.find(',', p);
+    if (e == std::string::npos) e = s.size();
+    c3_combo c{};
+    unsigned long long i = 0, r = 0, l = 0, q = 0;
+    if (std::sscanf(s.substr(p, e - p).c_str(), "%llu:%llu:%llu:%llu", &i, &r, &l, &q) != 4 || l == 0 || q == 0) {
+      std::fprintf(stderr, "ref_driver: bad combination '%s' (inserts:ranges:length:slot)\n",
+                   s.substr(p, e - p).c_str());
+      std::exit(2);
+    }
+    c = {i, r, l, q};
+    out.push_back(c);
+    p = e + 1;
+  }
+  return out;
+}
+
+void range_checksums(const std::vector<uint32_t>& cnt, const pair_t* dpairs, uint64_t slot, uint64_t& cs_c,
+                     uint64_t& cs_p, uint64_t& max_count) {
+  auto pairs = host_copy(dpairs, cnt.size() * slot);
+  cs_c = cs_p = max_count = 0;
+  for (uint64_t i = 0; i < cnt.size(); ++i) {
+    cs_c += count_term(i, cnt[i]);
+    max_count = std::max<uint64_t>(max_count, cnt[i]);
+    const uint64_t m = std::min<uint64_t>(cnt[i], slot);
+    for (uint64_t j = 0; j < m; ++j) cs_p += pair_term(i, j, pairs[i * slot + j].first, pairs[i * slot + j].second);
+  }
+}
+
+int run_c3(const args_t& a) {
+  const uint64_t n      = a.initial;
+  const uint64_t stride = a.stride ? a.stride : 0xFFFFFFFDull / std::max<uint64_t>(n, 1);
+  const auto combos     = parse_combos(a.combos);
+  std::vector<uint32_t> keys(n), vals(n);
+  mvbt_wl_distinct_keys(a.seed, 0, n, keys.data());
+  mvbt_wl_values(keys.data(), n, (uint32_t)a.seed, vals.data());
+  for (const auto& c : combos) {
+    if (4 * (n / 6 + 1) + 4 * c.inserts + 1024 > kPoolNodes) {
+      std::fprintf(stderr, "ref_driver: workload could exceed the %llu-node pool\n",
+                   (unsigned long long)kPoolNodes);
+      return 2;
+    }
+  }
+  uint32_t *dk = dev_copy(keys), *dv = dev_copy(vals);
+  cudaEvent_t e0, e1, e2;
+  check(cudaEventCreate(&e0), "event");
+  check(cudaEventCreate(&e1), "event");
+  check(cudaEventCreate(&e2), "event");
+  const uint32_t reps = std::max(1u, a.reps);
+  std::printf("{\"mode\": \"c3\", \"initial\": %llu, \"seed\": %llu, \"stride\": %llu, \"reps\": %u, \"runs\": [",
+              (unsigned long long)n, (unsigned long long)a.seed, (unsigned long long)stride, reps);
+  for (size_t ci = 0; ci < combos.size(); ++ci) {
+    const c3_combo& c = combos[ci];
+    std::vector<uint32_t> ins(c.inserts), ivals(c.inserts), lo(c.ranges), hi(c.ranges);
+    mvbt_wl_distinct_keys(a.seed, n, c.inserts, ins.data());
+    mvbt_wl_values(ins.data(), c.inserts, (uint32_t)a.seed, ivals.data());
+    mvbt_wl_uniform_keys(a.seed + 1, c.ranges, lo.data());
+    mvbt_wl_upper_bounds(lo.data(), c.ranges, c.length, stride, hi.data());
+    uint32_t *di = dev_copy(ins), *div = dev_copy(ivals), *dlo = dev_copy(lo), *dhi = dev_copy(hi);
+    const uint64_t tail = c.length * stride;
+    pair_t* dp          = dev_alloc<pair_t>(c.ranges * c.slot + tail);
+    double ins_ms = 0, ops_ms = 0;
+    for (uint32_t r = 0; r < a.warmup + reps; ++r) {  // fresh tree per experiment
+      vtree_t tree;
+      check(cudaDeviceSynchronize(), "setup");
+      check(cudaEventRecord(e0, 0), "record");
+      tree.insert(dk, dv, (uint32_t)n, 0, true);
+      check(cudaEventRecord(e1, 0), "record");
+      tree.concurrent_insert_range(di, div, (uint32_t)c.inserts, dlo, dhi, (uint32_t)c.ranges, dp,
+                                   (uint32_t)c.slot, 0);
+      check(cudaEventRecord(e2, 0), "record");
+      check(cudaEventSynchronize(e2), "sync");
+      check(cudaGetLastError(), "concurrent_insert_range");
+      if (r < a.warmup) continue;
+      ins_ms += elapsed_ms(e0, e1);
+      ops_ms += elapsed_ms(e1, e2);
+    }
+    cudaFree(dp);
+    ins_ms /= reps;
+    ops_ms /= reps;
+    // sums[f][4]: f = 0 second insert in place (ViB), f = 1 out of place (VoB)
+    uint64_t sums[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}}, maxc = 0;
+    const uint64_t cslot = 4 * c.length + 64;
+    if (a.checksums) {
+      pair_t* dq     = dev_alloc<pair_t>(c.ranges * cslot + tail);
+      uint32_t* dcnt = dev_alloc<uint32_t>(c.ranges);
+      for (int f = 0; f < 2; ++f) {
+        vtree_t tree;
+        tree.insert(dk, dv, (uint32_t)n, 0, true);
+        const uint32_t S0 = tree.take_snapshot();
+        tree.insert(di, div, (uint32_t)c.inserts, 0, f == 0);
+        const uint32_t S1 = tree.take_snapshot();
+        const uint32_t S[2] = {S0, S1};
+        for (int v = 0; v < 2; ++v) {
+          check(cudaMemset(dq, 0xFF, (c.ranges * cslot + tail) * sizeof(pair_t)), "memset");
+          tree.range_query(dlo, dhi, dq, dcnt, (uint32_t)cslot, (uint32_t)c.ranges, S[v], 0, false);
+          check(cudaDeviceSynchronize(), "range_query");
+          check(cudaGetLastError(), "range_query");
+          const auto cnt = host_copy(dcnt, c.ranges);
+          uint64_t m = 0;
+          range_checksums(cnt, dq, cslot, sums[f][2 * v], sums[f][2 * v + 1], m);
+          maxc = std::max(maxc, m);
+          if (!a.dump.empty()) {  // raw uint32 counts, one file per insert form and snapshot
+            const std::string path = a.dump + (f ? "_vob_s" : "_vib_s") + std::to_string(v) + ".u32";
+            FILE* fp = std::fopen(path.c_str(), "wb");
+            if (fp) {
+              std::fwrite(cnt.data(), sizeof(uint32_t), cnt.size(), fp);
+              std::fclose(fp);
+            }
+          }
+        }
+      }
+      cudaFree(dq);
+      cudaFree(dcnt);
+    }
+    std::printf("%s{\"inserts\": %llu, \"ranges\": %llu, \"length\": %llu, \"slot\": %llu, \"insert_ms\": %.4f, "
+                "\"ops_ms\": %.4f, \"insert_mops\": %.3f, \"ops_mops\": %.3f, \"check_slot\": %llu, "
+                "\"max_count\": %llu, \"checksums\": [%llu, %llu, %llu, %llu], "
+                "\"checksums_out_of_place\": [%llu, %llu, %llu, %llu]}",
+                ci ? ", " : "", (unsigned long long)c.inserts, (unsigned long long)c.ranges,
+                (unsigned long long)c.length, (unsigned long long)c.slot, ins_ms, ops_ms, n / (ins_ms * 1e3),
+                (c.inserts + c.ranges) / (ops_ms * 1e3), (unsigned long long)cslot, (unsigned long long)maxc,
+                (unsigned long long)sums[0][0], (unsigned long long)sums[0][1], (unsigned long long)sums[0][2],
+                (unsigned long long)sums[0][3], (unsigned long long)sums[1][0], (unsigned long long)sums[1][1],
+                (unsigned long long)sums[1][2], (unsigned long long)sums[1][3]);
+    std::fflush(stdout);
+    for (uint32_t* p : {di, div, dlo, dhi}) cudaFree(p);
+  }
+  std::printf("]}\n");
+  cudaFree(dk);
+  cudaFree(dv);
   return 0;
 }
 
@@ -417,6 +666,8 @@ int run_c4(const args_t& a) {
 int main(int argc, char** argv) {
   args_t a = parse(argc, argv);
   if (a.mode == "c1") return run_c1(a);
+  if (a.mode == "c2") return run_c2(a);
+  if (a.mode == "c3") return run_c3(a);
   if (a.mode == "c4") return run_c4(a);
   std::fprintf(stderr, "ref_driver: unknown mode %s\n", a.mode.c_str());
   return 2;

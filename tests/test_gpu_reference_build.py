@@ -4,6 +4,10 @@ oracle/_ref/ref_driver (built by oracle/ref_build.py from the reference's unmodi
 the reference through its public host API; this library runs the same workload through its C ABI;
 checksums of every find result, range count and range pair are compared (tests/refbuild.py).
   * C1 shape: plain B-link tree, insert then finds (half present, half never inserted).
+  * C2 shape: versioned tree, finds of the same queries at a snapshot before and after updates.
+  * C3 shape: versioned tree, range queries at a snapshot before and after new inserts (the
+    reference's concurrent_insert_range results depend on timing, so the check uses the
+    deterministic sequence).
   * C4 shape: versioned tree, mixed batches with one snapshot per batch. The reference issues each
     batch in its plain form (take_snapshot, find(ts), range_query(ts), insert, erase); this library
     runs all batches in one persistent launch. A final snapshot reads the whole key space.
@@ -100,3 +104,105 @@ def test_mixed_batches_match_reference_build(torch, w):
              pairs_sum(idx, np.minimum(cnt, slot), idx * slot, host(pairs).reshape(-1, 2))]
     assert final == ref["final"]
     assert int(cnt.sum()) == live
+
+
+@pytest.mark.parametrize("w", [8, 16])
+def test_versioned_finds_at_two_snapshots_match_reference_build(torch, w):
+    """C2 shape: insert, snapshot S0, in-place updates of an eighth of the keys, snapshot S1,
+    the same hit/miss queries at S0 and at S1."""
+    from mvgpubtree_b200 import workload as wl
+    import mvgpubtree_b200 as mv
+    n, seed = 1 << 17, 13
+    u = n // 8
+    ref = run_driver("c2", "--initial", str(n), "--updates", str(u), "--seed", str(seed))
+    keys = wl.distinct_keys(seed, 0, n)
+    upd = wl.shuffle(seed + 3, keys)[:u]
+    hits = wl.shuffle(seed + 1, keys)[: n // 2]
+    miss = wl.distinct_keys(seed, wl.MISS_INDEX_BASE, n - n // 2)
+    q = wl.shuffle(seed + 2, np.concatenate([hits, miss]))
+    t = mv.gpu_versioned_btree(pool_bytes=1 << 28, tile_width=w)
+    t.insert(dev(torch, keys), dev(torch, wl.values_for(keys, seed)))
+    s0 = t.take_snapshot()
+    t.insert(dev(torch, upd), dev(torch, wl.values_for(upd, seed ^ 1)))
+    s1 = t.take_snapshot()
+    sums = []
+    for s in (s0, s1):
+        out = torch.empty(n, dtype=torch.int32, device="cuda")
+        t.find(dev(torch, q), out, timestamp=s)
+        sums.append(find_sum(np.arange(n), host(out)))
+    assert t.check_errors() == 0
+    assert sums == ref["find_checksums"]
+
+
+def c3_case(seed, n, ops, u, L):
+    from mvgpubtree_b200 import workload as wl
+    stride = wl.stride_for(n)
+    n_ins = int(ops * u)
+    n_rq = ops - n_ins
+    keys = wl.distinct_keys(seed, 0, n)
+    ins = wl.distinct_keys(seed, n, n_ins)
+    lo = wl.uniform_keys(seed + 1, n_rq)
+    return dict(stride=stride, n_ins=n_ins, n_rq=n_rq, keys=keys, vals=wl.values_for(keys, seed), ins=ins,
+                ivals=wl.values_for(ins, seed), lo=lo, hi=wl.upper_bounds(lo, L, stride))
+
+
+def range_sums(cnt, pairs, slot):
+    idx = np.arange(cnt.size)
+    return [count_sum(idx, cnt), pairs_sum(idx, np.minimum(cnt, slot), idx * slot, pairs.reshape(-1, 2))]
+
+
+@pytest.mark.parametrize("w", [8, 16])
+@pytest.mark.parametrize("u,L", [(0.5, 8), (0.9, 128)])
+def test_insert_then_ranges_match_reference_build(torch, w, u, L, tmp_path):
+    """C3 shape: insert, snapshot S0, new keys inserted, snapshot S1, the same range queries at S0
+    and at S1 (4L + 64 pairs per query, more than any of these queries returns). The reference's
+    concurrent_insert_range results depend on timing, so the check is this deterministic sequence;
+    the driver also runs concurrent_insert_range on the same inputs (its timing path).
+
+    This library and the oracle agree on every query. The reference agrees with both when its
+    second insert is in place (its ViB form). With the out-of-place form (VoB) its range counts
+    at S0 include some keys inserted after S0 (1-3 extra in ~0.02-3 % of queries here); at S1 it
+    agrees. That case is recorded as an expected failure of the reference, not of this library."""
+    import mvgpubtree_b200 as mv
+    import oracle
+    n, seed, ops = 1 << 18, 29, 60_000
+    c = c3_case(seed, n, ops, u, L)
+    ref = run_driver("c3", "--initial", str(n), "--seed", str(seed), "--stride", str(c["stride"]),
+                     "--combos", f"{c['n_ins']}:{c['n_rq']}:{L}:{2 * L}",
+                     "--dump", str(tmp_path / "ref"))["runs"][0]
+    slot = 4 * L + 64
+    assert ref["check_slot"] == slot and ref["max_count"] <= slot
+    t = mv.gpu_versioned_btree(pool_bytes=1 << 28, tile_width=w)
+    t.insert(dev(torch, c["keys"]), dev(torch, c["vals"]))
+    s0 = t.take_snapshot()
+    t.insert(dev(torch, c["ins"]), dev(torch, c["ivals"]))
+    s1 = t.take_snapshot()
+    ours = []
+    for s in (s0, s1):
+        pairs = torch.full((c["n_rq"] * slot * 2,), -1, dtype=torch.int32, device="cuda")
+        counts = torch.empty(c["n_rq"], dtype=torch.int32, device="cuda")
+        t.range_query(dev(torch, c["lo"]), dev(torch, c["hi"]), pairs, counts, slot, c["n_rq"], s)
+        ours += range_sums(host(counts), host(pairs), slot)
+    assert t.check_errors() == 0
+    m = oracle.MVMap(True)
+    m.insert(c["keys"], c["vals"])
+    o0 = m.take_snapshot()
+    m.insert(c["ins"], c["ivals"])
+    o1 = m.take_snapshot()
+    expect, oc = [], []
+    for s in (o0, o1):
+        pairs, counts = m.range_query(c["lo"], c["hi"], slot, s)
+        expect += range_sums(counts, pairs, slot)
+        oc.append(counts)
+    assert ours == expect
+    assert ref["checksums"] == ours  # reference, second insert in place
+    vob = ref["checksums_out_of_place"]
+    assert vob[2:] == ours[2:]  # reference, out of place: at S1
+    if vob[:2] != ours[:2]:
+        rc = np.fromfile(tmp_path / "ref_vob_s0.u32", np.uint32)
+        bad = np.nonzero(rc != oc[0])[0]
+        extra = rc[bad].astype(np.int64) - oc[0][bad].astype(np.int64)
+        newer = oc[1][bad].astype(np.int64) - oc[0][bad].astype(np.int64)
+        assert np.all(extra > 0) and np.all(extra <= newer), "the reference's extra keys are not later inserts"
+        pytest.xfail(f"reference out-of-place insert: {bad.size} of {c['n_rq']} range counts at the earlier "
+                     f"snapshot include {int(extra.min())}-{int(extra.max())} keys inserted after it")
