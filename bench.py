@@ -21,7 +21,8 @@ serving  : continuous batching of Poisson-arriving requests (lognormal sizes, me
            throughput, beside the plain mode with one request per launch on an identical tree.
 configs  : the other workloads of the reference's benchmarks, measured alone before the above:
            c1 plain-tree insert + finds (2^20 keys), c2 versioned insert / update / finds at two
-           snapshots (2^25 keys), c3 concurrent insert + range on 40M keys (9 mixes).
+           snapshots (2^25 keys), c3 inserts + range queries at the snapshot before them on 40M
+           keys (9 mixes; one concurrent_insert_range call, and insert then range_query).
 
 With --impl reference the script times the reference implementation's own CUDA build
 (oracle/_ref/ref_driver, built by oracle/ref_build.py from the reference's unmodified headers) on
@@ -541,12 +542,17 @@ REF_DRIVER = Path(__file__).resolve().parent / "oracle" / "_ref" / "ref_driver"
 #   c1: plain B-link tree, 2^20 keys inserted, 2^20 finds (half hits)
 #   c2: versioned tree, 2^25 keys, 2^22 in-place updates, 2^25 finds at the snapshot before and
 #       at the snapshot after the updates
-#   c3: versioned tree of 40M keys, 10M ops in one concurrent_insert_range call (each op an insert
-#       with probability u, else a range query of length L), u in {5, 50, 90} %, L in {8, 32, 128}
+#   c3: versioned tree of 40M keys, 10M ops (each an insert with probability u, else a range query
+#       of length L at the snapshot taken before the inserts), u in {5, 50, 90} %, L in {8, 32, 128};
+#       "concurrent" = one concurrent_insert_range call, "sequence" = insert, then range_query
 # Every phase is timed alone with CUDA events, after one untimed experiment, mean of --config-reps.
 # ------------------------------------------------------------------------------------------------
 C1_KEYS, C2_KEYS, C2_UPDATES = 1 << 20, 1 << 25, 1 << 22
 C3_OPS, C3_UPDATE, C3_LENGTHS = 10_000_000, (0.05, 0.5, 0.9), (8, 32, 128)
+C3_REF_CONCURRENT_UNAVAILABLE = (
+    "the reference's concurrent_insert_range raised an illegal memory access on a B200 with "
+    "in-bounds inputs (262144 keys, 54000 inserts + 6000 range queries of L = 128), so it is not "
+    "run; its plain form (insert, then range_query at the snapshot before) is timed instead")
 
 
 def hit_miss_queries(wl, seed: int, keys: np.ndarray) -> np.ndarray:
@@ -672,24 +678,35 @@ def run_configs_ours(args) -> dict:
         insert_mops[w] = round(N / (sum(ms[1:]) / reps) / 1e3, 1)
     del dk, dv
     runs = {8: {}, 16: {}}
+    seq = {8: {}, 16: {}}
     for u, L, n_ins, n_rq in c3_combos(seed):
         ins = wl.distinct_keys(seed, N, n_ins)
         lo = wl.uniform_keys(seed + 1, n_rq)
         di, div, dlo, dhi = dev(ins), dev(wl.values_for(ins, seed)), dev(lo), dev(wl.upper_bounds(lo, L, stride))
         pairs = torch.empty(n_rq * 2 * L * 2, dtype=torch.int32, device="cuda")
+        counts = torch.empty(n_rq, dtype=torch.int32, device="cuda")
+        name = f"u{int(u * 100)}_L{L}"
+
+        def sequence(t):
+            s = t.take_snapshot()
+            return [timed(lambda: (t.insert(di, div), t.range_query(dlo, dhi, pairs, counts, 2 * L, n_rq, s)))]
+
         for w in (8, 16):
             ms = mean_runs(lambda: base[w].clone(),
                            lambda t: [timed(lambda: t.concurrent_insert_range(
                                di, div, n_ins, dlo, dhi, n_rq, pairs, 2 * L))])
-            runs[w][f"u{int(u * 100)}_L{L}"] = round(C3_OPS / ms[0] / 1e3, 1)
-        del di, div, dlo, dhi, pairs
+            runs[w][name] = round(C3_OPS / ms[0] / 1e3, 1)
+            ms = mean_runs(lambda: base[w].clone(), sequence)
+            seq[w][name] = round(C3_OPS / ms[0] / 1e3, 1)
+        del di, div, dlo, dhi, pairs, counts
         torch.cuda.empty_cache()
     for t in base.values():
         t.close()
     w = max(runs, key=lambda k: _hmean(list(runs[k].values())))
-    out["c3_concurrent_insert_range_40M"] = {
-        "tile_width": w, "insert_40M_mops": insert_mops[w], "ops_mops": runs[w],
-        "ops_hmean_mops": round(_hmean(list(runs[w].values())), 1)}
+    out["c3_insert_range_40M"] = {
+        "tile_width": w, "insert_40M_mops": insert_mops[w],
+        "concurrent_mops": runs[w], "concurrent_hmean_mops": round(_hmean(list(runs[w].values())), 1),
+        "sequence_mops": seq[w], "sequence_hmean_mops": round(_hmean(list(seq[w].values())), 1)}
     torch.cuda.empty_cache()
     return out
 
@@ -719,9 +736,11 @@ def run_configs_reference(args) -> dict:
         spec = ",".join(f"{i}:{r}:{L}:{2 * L}" for _, L, i, r in combos)
         c3 = drive("c3", "--initial", str(args.initial_keys), "--combos", spec, "--checksums", "0")
         ops = {f"u{int(u * 100)}_L{L}": round(x["ops_mops"], 1) for (u, L, _, _), x in zip(combos, c3["runs"])}
-        res["c3_concurrent_insert_range_40M"] = {
+        res["c3_insert_range_40M"] = {
             "insert_40M_mops": round(statistics.mean(x["insert_mops"] for x in c3["runs"]), 1),
-            "ops_mops": ops, "ops_hmean_mops": round(_hmean(list(ops.values())), 1)}
+            "concurrent_mops": None,
+            "concurrent_unavailable": C3_REF_CONCURRENT_UNAVAILABLE,
+            "sequence_mops": ops, "sequence_hmean_mops": round(_hmean(list(ops.values())), 1)}
     except (RuntimeError, subprocess.TimeoutExpired) as e:
         res["error"] = str(e)[-300:]
     return res

@@ -24,6 +24,7 @@ extern "C" int mvbt_internal_view(mvbt_tree* t, device_tree* view, int* tile_wid
                                   int* num_sms, uint32_t* blocks_per_sm, uint32_t* max_blocks,
                                   void** control);
 extern "C" void mvbt_internal_set_error(const char* msg);
+extern "C" void mvbt_internal_note_growth(mvbt_tree* t, uint64_t keys);
 
 struct mvbt_batch_plan {
   mvbt_tree* tree;
@@ -394,6 +395,7 @@ int mvbt_internal_batch_enqueue(mvbt_batch_plan* p, uint32_t num_batches, const 
   void* ctl;
   int st = mvbt_internal_view(p->tree, &c.view, &c.W, &c.block, &c.sms, &c.bps, &c.maxb, &ctl);
   if (st) return st;
+  mvbt_internal_note_growth(p->tree, total);  // an upper bound on the batches' inserts
   if (p->tile_width) c.W = p->tile_width;
   if (p->blocks_per_sm >= 0) c.bps = (uint32_t)p->blocks_per_sm;
   c.ctl = static_cast<mvbt::control_block*>(ctl);
@@ -427,6 +429,7 @@ int mvbt_batch_run(mvbt_batch_plan* p, uint32_t num_batches, const uint64_t* bat
   void* ctl;
   int st = mvbt_internal_view(p->tree, &c.view, &c.W, &c.block, &c.sms, &c.bps, &c.maxb, &ctl);
   if (st) return st;
+  mvbt_internal_note_growth(p->tree, total);  // an upper bound on the batches' inserts
   if (p->tile_width) c.W = p->tile_width;
   if (p->blocks_per_sm >= 0) c.bps = (uint32_t)p->blocks_per_sm;
   c.ctl = static_cast<mvbt::control_block*>(ctl);
@@ -632,6 +635,7 @@ extern "C" int mvbt_batch_run_noalloc(mvbt_tree* tree, uint32_t num_batches, con
   int st = mvbt_internal_view(tree, &c.view, &c.W, &c.block, &c.sms, &c.bps, &c.maxb, &ctl);
   if (st) return st;
   if (!c.view.versioned) return fail(MVBT_ERR_NOT_SUPPORTED, "mixed batches need a versioned tree");
+  mvbt_internal_note_growth(tree, num_ops);  // an upper bound on the batches' inserts
   c.ctl = static_cast<mvbt::control_block*>(ctl);
   int dev = 0;
   MVBT_TRY(cudaGetDevice(&dev));
