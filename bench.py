@@ -335,14 +335,25 @@ def run_ours(args, dist: Dist):
     h_total = torch.zeros(len(e2e_steps), dtype=torch.int64).pin_memory()
     s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream()
 
+    # per-step stage marks (CUDA events on each stage's stream): input copy, run + packing, output
+    # copy; and the host's wait for each step's pair count
+    tev = lambda: torch.cuda.Event(enable_timing=True)
+    marks = [{k: tev() for k in ("in0", "in1", "k0", "k1", "o0", "o1")} for _ in e2e_steps]
+    host_wait = [0.0] * len(e2e_steps)
+    host_run = [0.0] * len(e2e_steps)
+
     def finish(q):
         bq, b = bufs[q % 2], e2e_steps[q]
+        t0 = time.perf_counter()
         bq["ev_k"].synchronize()  # step q's run and packing are done; its pair count is on the host
+        host_wait[q] = 1e3 * (time.perf_counter() - t0)
         tot = int(h_total[q])
         with torch.cuda.stream(s_out):
             s_out.wait_event(bq["ev_k"])
+            marks[q]["o0"].record(s_out)
             bq["h_res"][: b.num_ops].copy_(bq["res"][: b.num_ops], non_blocking=True)
             bq["h_comp"][: 2 * tot].copy_(bq["comp"][: 2 * tot], non_blocking=True)
+            marks[q]["o1"].record(s_out)
             bq["ev_out"].record(s_out)
         return b.num_ops * 4 + 8 + tot * 8
 
@@ -357,17 +368,23 @@ def run_ours(args, dist: Dist):
             ev0.record(stream)
         with torch.cuda.stream(s_in):
             s_in.wait_event(bs["ev_k"])  # the run two steps back has read these buffers
+            marks[s]["in0"].record(s_in)
             dst = [bs["ops"][0][:n], bs["ops"][1][:n], bs["ops"][2][:n], bs["off"][:n], bs["cap"][:n]]
             for d, h in zip(dst, h_in[s]):
                 d.copy_(h, non_blocking=True)
+            marks[s]["in1"].record(s_in)
             bs["ev_in"].record(s_in)
         stream.wait_event(bs["ev_in"])
         stream.wait_event(bs["ev_out"])  # its results from two steps back have crossed
+        marks[s]["k0"].record(stream)
+        t_run = time.perf_counter()
         bs["plan"].run(b.batch_off, bs["ops"][0], bs["ops"][1], bs["ops"][2], bs["off"], bs["cap"], bs["res"],
                        bs["rout"], mode=mv.BATCH_GRAPH, stream=stream)
         # the pair count goes straight to pinned host memory: no copy queued behind the big ones
         bs["plan"].compact_ranges(n, bs["ops"][0], bs["res"], bs["off"], bs["cap"], bs["rout"], bs["comp"],
                                   h_total[s:s + 1], stream=stream)
+        host_run[s] = 1e3 * (time.perf_counter() - t_run)
+        marks[s]["k1"].record(stream)
         bs["ev_k"].record(stream)
         if s >= We:
             h2d += sum(int(h.numel() * h.element_size()) for h in h_in[s])
@@ -382,6 +399,14 @@ def run_ours(args, dist: Dist):
     e2e_ms = dist.max(ev0.elapsed_time(ev1))
     e2e_ops = sum(b.num_ops for b in e2e_steps[We:]) * dist.world
     e2e_value = e2e_ops / (e2e_ms * 1e-3) / 1e6
+    e2e_stages = [{"in_ms": round(m["in0"].elapsed_time(m["in1"]), 2),
+                   "run_ms": round(m["k0"].elapsed_time(m["k1"]), 2),
+                   "out_ms": round(m["o0"].elapsed_time(m["o1"]), 2),
+                   "run_start_ms": round(ev0.elapsed_time(m["k0"]), 2),
+                   "gap_before_run_ms": round(marks[i - 1]["k1"].elapsed_time(m["k0"]), 2),
+                   "host_run_call_ms": round(host_run[i], 2),
+                   "host_wait_ms": round(host_wait[i], 2)}
+                  for i, m in enumerate(marks) if i >= We]
 
     # ---- roofline of the persistent kernel ----
     rep = trees["batched"].validate_tree_structure()
@@ -428,7 +453,8 @@ def run_ours(args, dist: Dist):
                 "h2d_bytes_per_step": int(h2d / max(1, Ke)), "d2h_bytes_per_step": int(d2h / max(1, Ke)),
                 "mode": "CUDA graph replay via the public batch API, pinned host buffers, two steps in "
                         "flight: op arrays in, results and the range pairs that exist (packed by "
-                        "mvbt_batch_compact_ranges) back, overlapping the next step's run"},
+                        "mvbt_batch_compact_ranges) back, overlapping the next step's run",
+                "stages": e2e_stages},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": traffic,
                      "kernel": "k_batched", "kernel_ms": round(avg_kms, 3),

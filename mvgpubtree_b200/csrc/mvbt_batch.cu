@@ -367,6 +367,9 @@ int mvbt_batch_plan_destroy(mvbt_batch_plan* p) {
 // slot's previous launch has completed.
 uint64_t* mvbt_internal_plan_staging(mvbt_batch_plan* p) { return p->h_batch_off; }
 
+// Most ops one run of the plan holds (mvbt_compact.cu sizes its scratch for it on first use).
+uint64_t mvbt_internal_plan_max_ops(mvbt_batch_plan* p) { return p ? p->max_ops : 0; }
+
 // Device scratch of at least `bytes` owned by the plan (mvbt_compact.cu); grows by reallocation
 // after the device is idle, so callers allocate it once, outside any timed region, by a first call.
 void* mvbt_internal_plan_scratch(mvbt_batch_plan* p, uint64_t bytes) {

@@ -16,6 +16,7 @@
 
 extern "C" void mvbt_internal_set_error(const char* msg);
 extern "C" void* mvbt_internal_plan_scratch(mvbt_batch_plan* p, uint64_t bytes);
+extern "C" uint64_t mvbt_internal_plan_max_ops(mvbt_batch_plan* p);
 
 namespace {
 
@@ -127,7 +128,12 @@ extern "C" int mvbt_batch_compact_ranges(mvbt_batch_plan* plan, uint64_t n, cons
     return e == cudaSuccess ? MVBT_OK : fail(MVBT_ERR_CUDA, cudaGetErrorString(e));
   }
   const uint64_t tiles = (n + kTile - 1) / kTile;
-  auto* scratch = static_cast<uint64_t*>(mvbt_internal_plan_scratch(plan, (n + tiles) * sizeof(uint64_t)));
+  // Scratch for the most ops the plan holds, so it is allocated once, by the first call: growing
+  // it later reallocates after a device-wide synchronisation, which would stall a pipelined
+  // caller on every step larger than the ones before.
+  const uint64_t cap_n     = std::max<uint64_t>(n, mvbt_internal_plan_max_ops(plan));
+  const uint64_t cap_tiles = (cap_n + kTile - 1) / kTile;
+  auto* scratch = static_cast<uint64_t*>(mvbt_internal_plan_scratch(plan, (cap_n + cap_tiles) * sizeof(uint64_t)));
   if (!scratch) return fail(MVBT_ERR_OUT_OF_MEMORY, "compact ranges: scratch allocation failed");
   uint64_t* off      = scratch;
   uint64_t* tile_sum = scratch + n;
