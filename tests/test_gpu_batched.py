@@ -116,3 +116,38 @@ def test_compact_range_output_packs_the_pairs_that_exist(torch, dest):
     assert got_total == len(want) and got_total > 0
     got = comp.cpu().numpy().view(np.uint32).reshape(-1, 2)[:got_total]
     assert np.array_equal(got, want)
+
+
+def test_compact_ranges_in_a_larger_plan_for_growing_op_counts(torch):
+    """The packing scratch is sized for the plan's largest run on first use: packing a prefix of
+    the ops and then all of them on a plan that holds more ops gives the right pairs both times."""
+    from mvgpubtree_b200 import workload as wl
+    import mvgpubtree_b200 as mv
+    initial, seed = 100_000, 31
+    init = wl.distinct_keys(seed, 0, initial)
+    t = mv.gpu_versioned_btree(pool_bytes=1 << 28)
+    t.insert(torch.from_numpy(init.view(np.int32)).cuda(), torch.from_numpy(wl.values_for(init, 0).view(np.int32)).cuda())
+    gen = wl.MixGenerator(seed, initial, stride=wl.stride_for(initial), batch_median=4096.0,
+                          batch_min=256, batch_max=32768)
+    b = gen.generate(12)
+    d = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.int64 if a.dtype == np.uint64 else np.int32)).cuda()
+    ops = [d(b.type), d(b.key), d(b.arg), d(b.out_off), d(b.range_cap)]
+    res = torch.empty(b.num_ops, dtype=torch.int32, device="cuda")
+    rout = torch.full((b.range_pairs * 2,), -1, dtype=torch.int32, device="cuda")
+    plan = t.batch_plan(4 * b.num_ops, 12)
+    plan.run(b.batch_off, *ops, res, rout)
+    torch.cuda.synchronize()
+    r = res.cpu().numpy().view(np.uint32)
+    ro = rout.cpu().numpy().view(np.uint32).reshape(-1, 2)
+    for n in (int(b.batch_off[6]), b.num_ops):
+        comp = torch.full((b.range_pairs * 2,), -1, dtype=torch.int32, device="cuda")
+        total = torch.zeros(1, dtype=torch.int64, device="cuda")
+        plan.compact_ranges(n, ops[0], res, ops[3], ops[4], rout, comp, total)
+        torch.cuda.synchronize()
+        rq = np.nonzero(b.type[:n] == 3)[0]
+        want = np.concatenate([ro[int(b.out_off[i]): int(b.out_off[i]) + min(int(r[i]), int(b.range_cap[i]))]
+                               for i in rq]) if rq.size else np.zeros((0, 2), np.uint32)
+        got_total = int(total.cpu().numpy()[0])
+        assert got_total == len(want), n
+        assert np.array_equal(comp.cpu().numpy().view(np.uint32).reshape(-1, 2)[:got_total], want), n
+    assert t.check_errors() == 0
