@@ -196,13 +196,25 @@ struct control_block {
   unsigned long long stat_reused;       // nodes handed out again from the free ring
   unsigned long long ring_fail;  // first ring position of a failed chunk pop (~0: none)
   unsigned long long free_mark;  // ring head at the end of the last pass (for stat_reused)
+  // Per-SM shares of the copy and split counts ([slot][0] copies, [slot][1] splits), one 128-B
+  // line per SM slot: the counting atomics of different SMs land on different lines instead of
+  // all on one word. stat_cow / stat_split stay 0; a count is its slots' sum (stat_total).
+  unsigned long long sm_stats[kMaxSmSlots][16];
 };
+
 
 #if defined(MVBT_HOST_EMULATION)
 #define MVBT_HD inline
 #else
 #define MVBT_HD __host__ __device__ __forceinline__
 #endif
+
+// Total of per-SM counter k (0 copies, 1 splits) plus the unsharded field.
+MVBT_HD unsigned long long stat_total(const control_block& c, int k) {
+  unsigned long long s = k == 0 ? c.stat_cow : c.stat_split;
+  for (int i = 0; i < kMaxSmSlots; ++i) s += c.sm_stats[i][k];
+  return s;
+}
 
 // Word t (0..63) of the initial tree. Node 0 is the anchor: an interior node whose only entry
 // {0 -> 1} points at the top of the tree, level 1. Node 1 is a leaf holding the tombstone {0, 0}.
@@ -246,6 +258,8 @@ MVBT_HD void init_control(control_block& c, uint32_t capacity, uint32_t chunk, u
   for (int i = 0; i < 16; ++i) c.err_site[i] = 0;
   // used == chunk: the first allocation on each SM refills its chunk from the bump pointer
   for (int i = 0; i < kMaxSmSlots; ++i) c.sm_pool[i] = chunk;
+  for (int i = 0; i < kMaxSmSlots; ++i)
+    for (int j = 0; j < 16; ++j) c.sm_stats[i][j] = 0;
   c.retire_log       = retire_log;
   c.free_ring        = free_ring;
   c.retire_head      = 0;
@@ -818,7 +832,7 @@ struct device_tree {
     if (reclaim)
       retire_logged(ctl, copy);
     else
-      atomicAdd(&ctl->stat_cow, 1ull);
+      atomicAdd(&ctl->sm_stats[sm_id() % kMaxSmSlots][0], 1ull);
   }
   // One entry of a reclaim pass over the retire log; no writer runs during a pass. A copy made in
   // epoch E is read only at snapshots below E, so with no live snapshot below the watermark M it
@@ -1299,7 +1313,7 @@ struct device_tree {
     store<W>(r, right, t);
     publish_fence(t);
     store<W>(idx, left, t);
-    if (t.thread_rank() == 0) atomicAdd(&ctl->stat_split, 1ull);
+    if (t.thread_rank() == 0) atomicAdd(&ctl->sm_stats[sm_id() % kMaxSmSlots][1], 1ull);
     release(idx, h, t);
     sep_key   = rmin;
     sep_child = r;
@@ -1336,7 +1350,7 @@ struct device_tree {
     h.ol = ((lvl + 1) << 28) | (h.ol & kIndexMask);
     set_header<W>(n, h, t);
     store<W>(kAnchor, n, t);
-    if (t.thread_rank() == 0) atomicAdd(&ctl->stat_split, 1ull);
+    if (t.thread_rank() == 0) atomicAdd(&ctl->sm_stats[sm_id() % kMaxSmSlots][1], 1ull);
     release(kAnchor, h, t);
     return true;
   }

@@ -949,7 +949,8 @@ int mvbt_stats(mvbt_tree* t, uint64_t* out, uint32_t n) {
   control_block c;
   MVBT_CUDA_TRY(cudaMemcpy(&c, t->ctl, sizeof(c), cudaMemcpyDeviceToHost));
   const bool rc  = c.reclaim_cap != 0;
-  uint64_t v[27] = {rc ? c.retire_tail : c.stat_cow, c.stat_split, c.stat_max_hops, c.stat_max_steps,
+  uint64_t v[27] = {rc ? c.retire_tail : mvbt::stat_total(c, 0), mvbt::stat_total(c, 1), c.stat_max_hops,
+                    c.stat_max_steps,
                     c.epoch, c.error};
   for (int i = 0; i < 16; ++i) v[6 + i] = c.err_site[i];
   v[22] = c.stat_restarts;

@@ -169,13 +169,13 @@ uint32_t emu_errors(void* h) { return static_cast<emu_tree*>(h)->ctl.error; }
 uint32_t emu_bump(void* h) { return static_cast<emu_tree*>(h)->ctl.bump; }
 void emu_stats(void* h, uint64_t* out) {
   auto& c = static_cast<emu_tree*>(h)->ctl;
-  out[0] = c.stat_cow;
-  out[1] = c.stat_split;
+  out[0] = mvbt::stat_total(c, 0);
+  out[1] = mvbt::stat_total(c, 1);
   out[2] = c.stat_max_hops;
   out[3] = c.stat_max_steps;
   for (int i = 0; i < 16; ++i) out[4 + i] = c.err_site[i];
   out[20] = c.stat_restarts;
-  out[21] = c.reclaim_cap ? c.retire_tail : c.stat_cow;
+  out[21] = c.reclaim_cap ? c.retire_tail : mvbt::stat_total(c, 0);
   out[22] = c.stat_reclaimed;
   const unsigned long long fh = c.ring_fail < c.free_head ? c.ring_fail : c.free_head;
   out[23] = c.reclaim_cap ? c.free_tail - fh : 0;
