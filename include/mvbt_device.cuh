@@ -1698,10 +1698,10 @@ MVBT_DEV void batched_worker(const device_tree& T, const batch_view& B, const ba
           }
           __threadfence();
           t.sync();
-          if (t.thread_rank() == 0) {
-            uint32_t c = atomicAdd(&sc.writes_done[b], 1u) + 1u;
-            if (c == sc.n_writes[b]) advance_done(sc, nb);
-          }
+          // Counted without reading the sum back (a reduction the tile does not wait for): the
+          // tiles that wait for a batch (wait_batch_ready) and the warps with nothing runnable
+          // advance done_batches.
+          if (t.thread_rank() == 0) atomicAdd(&sc.writes_done[b], 1u);
         }
       }
     }
