@@ -13,8 +13,12 @@ e2e      : Mops/s through the public batch API with host buffers: per step the o
            copied from pinned host memory, the captured CUDA graph is replayed, and the results
            (values, counts) and the range pairs that exist (packed on the device) are copied
            back; two steps are in flight, so copies overlap the next step's run.
-plain    : the same batches as one snapshot + one launch per batch (the drop-in method).
+plain    : the same W warm-up + K timed steps as one snapshot + one launch per batch (the drop-in
+           method), on an identical tree, so both arms time the same steps on trees of the same age.
 roofline : algorithmic bytes of the persistent kernel per launch / its CUDA-event time.
+verified : every result of every step, batched against plain (range pairs on the warm-up steps);
+           step 0 in full (find values, range counts and pairs) against the CPU oracle and against
+           the reference implementation's own CUDA build; configs 1-3 against the oracle.
 serving  : continuous batching of Poisson-arriving requests (lognormal sizes, median 256 ops) at
            offered loads of 10 / 50 / 200 M ops/s for a short window each, on a 40M-key tree with
            reclamation; p50 / p99 / p999 latency (arrival to results on the host) and achieved
@@ -28,8 +32,8 @@ With --impl reference the script times the reference implementation's own CUDA b
 (oracle/_ref/ref_driver, built by oracle/ref_build.py from the reference's unmodified headers) on
 the same batches through its public host API, one batch at a time (take_snapshot, find(ts),
 range_query(ts), insert, erase), and reports the oracle's multiversion ordered map
-(key-range partitioned over all host cores, bounded sample of every step) as its cpu_baseline.
-Without the reference build it times that CPU map instead.
+(key-range partitioned over all host cores, one full step) as its cpu_baseline. Without the
+reference build its value is null and the line says why.
 """
 from __future__ import annotations
 
@@ -67,11 +71,8 @@ def parse_args():
     ap.add_argument("--tile-width", type=int, default=8)
     ap.add_argument("--blocks-per-sm", type=int, default=0,
                     help="0 = full occupancy of the default kernel; 6 / 8 = register-capped variants")
-    ap.add_argument("--plain-steps", type=int, default=2)
     ap.add_argument("--e2e-steps", type=int, default=4)
     ap.add_argument("--pool-gb", type=float, default=24.0)
-    ap.add_argument("--cpu-sample-ops", type=int, default=4_000_000,
-                    help="ops of the bounded CPU-baseline sample per step")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep --tile-width / --blocks-per-sm instead of tuning the launch shape")
@@ -194,7 +195,7 @@ def measured_hbm_gbs():
 # workload
 # ------------------------------------------------------------------------------------------------
 def make_workload(seed: int, initial: int, steps: int, batches: int):
-    from mvgpubtree_b200 import workload as wl
+    import workload as wl
     t0 = time.time()
     init = wl.distinct_keys(seed, 0, initial)
     vals = wl.values_for(init, 0)
@@ -219,6 +220,19 @@ def op_bytes(b, result: np.ndarray, height: int, leaf_fill: float) -> float:
     return total
 
 
+def valid_pair_positions(torch, d_type, d_result, d_off, d_cap):
+    """Device positions (pair index into the step's range output) of every pair the step's range
+    queries wrote: query i's first min(count_i, cap_i) slots from out_off[i]."""
+    r = d_type == 3
+    off = d_off[r]
+    take = torch.minimum(d_result[r].long() & 0xFFFFFFFF, d_cap[r].long() & 0xFFFFFFFF)
+    total = int(take.sum())
+    if total == 0:
+        return torch.empty(0, dtype=torch.int64, device=d_type.device)
+    starts = torch.cumsum(take, 0) - take
+    return torch.repeat_interleave(off - starts, take) + torch.arange(total, device=d_type.device)
+
+
 def run_ours(args, dist: Dist):
     import torch
     import mvgpubtree_b200 as mv
@@ -227,9 +241,9 @@ def run_ours(args, dist: Dist):
     dist.init("nccl")
     seed = args.seed + 7919 * dist.rank
     W, K = max(3, args.warmup), args.steps
-    Wp, Kp = 1, max(1, args.plain_steps)
     We, Ke = 2, max(1, args.e2e_steps)  # e2e warm-up: one step per buffer set (graph capture, scratch)
-    n_steps = max(W + K, Wp + Kp) + We + Ke
+    V = min(W, 3)  # warm-up steps whose range pairs are compared between the batched and plain arms
+    n_steps = W + K + We + Ke
     init, vals, steps, gen_s = make_workload(seed, args.initial_keys, n_steps, args.batches)
 
     def dev(a):
@@ -256,57 +270,85 @@ def run_ours(args, dist: Dist):
     if not args.no_autotune:
         from mvgpubtree_b200.autotune import autotune_batches
         tune = autotune_batches(trees["batched"], steps[:2], plan=plans["batched"])
-    range_out = torch.empty(max(1, max_pairs) * 2, dtype=torch.int32, device="cuda")
+    range_out = {k: torch.empty(max(1, max_pairs) * 2, dtype=torch.int32, device="cuda") for k in trees}
     stream = torch.cuda.current_stream()
 
-    # ---- batched, device-resident: W warm-up + K timed steps, one persistent launch each ----
+    # Both arms run the same W warm-up + K timed steps on identical trees, so their timed steps
+    # meet trees of the same age. Results (find values, range counts) of every step are kept for
+    # the batched-vs-plain comparison; range pairs are compared on the first V warm-up steps.
     dsteps = [[dev(b.type), dev(b.key), dev(b.arg), dev(b.out_off), dev(b.range_cap)] for b in steps[: W + K]]
-    results = [torch.empty(b.num_ops, dtype=torch.int32, device="cuda") for b in steps[: W + K]]
+    results = {k: [torch.empty(b.num_ops, dtype=torch.int32, device="cuda") for b in steps[: W + K]]
+               for k in trees}
+    positions, saved_pairs, step0 = [], [], None
+
+    def run_arm(name, mode, on_warm):
+        plan = plans[name]
+        for s in range(W):
+            plan.run(steps[s].batch_off, *dsteps[s], results[name][s], range_out[name], mode=mode)
+            on_warm(s)
+        trees[name].check_errors()
+        plan.enable_timing(name == "batched")
+        clocks = ClockSampler(dist.local)
+        clocks.start()
+        dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for s in range(W, W + K):
+            plan.run(steps[s].batch_off, *dsteps[s], results[name][s], range_out[name], mode=mode)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        dist.barrier()
+        clk = clocks.stop()
+        kms = plan.kernel_times() if name == "batched" else []
+        plan.enable_timing(False)
+        trees[name].check_errors()
+        return dist.max(e0.elapsed_time(e1)), clk, kms
+
+    def batched_warm(s):
+        nonlocal step0
+        if s >= V:
+            return
+        d = dsteps[s]
+        pos = valid_pair_positions(torch, d[0], results["batched"][s], d[3], d[4])
+        positions.append(pos)
+        saved_pairs.append(range_out["batched"].view(-1, 2)[pos].clone())
+        if s == 0:  # the first full step, checked against the oracle and the reference build
+            n = steps[0].range_pairs
+            step0 = (results["batched"][0].cpu().numpy().view(np.uint32).copy(),
+                     range_out["batched"][: 2 * n].cpu().numpy().view(np.uint32).reshape(n, 2).copy())
+
+    pair_mismatch = []
+
+    def plain_warm(s):
+        if s < V:
+            got = range_out["plain"].view(-1, 2)[positions[s]]
+            pair_mismatch.append(int((got != saved_pairs[s]).any(dim=1).sum()))
+
+    # ---- batched, device-resident: W warm-up + K timed steps, one persistent launch each ----
     plan = plans["batched"]
-    for s in range(W):
-        plan.run(steps[s].batch_off, *dsteps[s], results[s], range_out, mode=mv.BATCH_PERSISTENT)
-    trees["batched"].check_errors()
-    plan.enable_timing(True)
-    clocks = ClockSampler(dist.local)
-    clocks.start()
-    dist.barrier()
-    torch.cuda.synchronize()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    ev0.record(stream)
-    for s in range(W, W + K):
-        plan.run(steps[s].batch_off, *dsteps[s], results[s], range_out, mode=mv.BATCH_PERSISTENT)
-    ev1.record(stream)
-    torch.cuda.synchronize()
-    dist.barrier()
-    clk = clocks.stop()
-    ms = ev0.elapsed_time(ev1)
-    kernel_ms = plan.kernel_times()
-    plan.enable_timing(False)
-    trees["batched"].check_errors()
+    ms_max, clk, kernel_ms = run_arm("batched", mv.BATCH_PERSISTENT, batched_warm)
     ops_timed = sum(steps[s].num_ops for s in range(W, W + K))
-    ms_max = dist.max(ms)
     ops_all = ops_timed * dist.world
     value = ops_all / (ms_max * 1e-3) / 1e6
 
-    # ---- plain: one snapshot + one launch per batch, same batches on an identical tree ----
-    pplan = plans["plain"]
-    for s in range(Wp):
-        pplan.run(steps[s].batch_off, *dsteps[s], results[s], range_out, mode=mv.BATCH_PER_LAUNCH)
-    dist.barrier()
-    torch.cuda.synchronize()
-    ev0.record(stream)
-    for s in range(Wp, Wp + Kp):
-        pplan.run(steps[s].batch_off, *dsteps[s], results[s], range_out, mode=mv.BATCH_PER_LAUNCH)
-    ev1.record(stream)
-    torch.cuda.synchronize()
-    trees["plain"].check_errors()
-    plain_ms = dist.max(ev0.elapsed_time(ev1))
-    plain_ops = sum(steps[s].num_ops for s in range(Wp, Wp + Kp)) * dist.world
-    plain_value = plain_ops / (plain_ms * 1e-3) / 1e6
+    # ---- plain: one snapshot + one launch per batch, the same steps on an identical tree ----
+    plain_ms, plain_clk, _ = run_arm("plain", mv.BATCH_PER_LAUNCH, plain_warm)
+    plain_value = ops_all / (plain_ms * 1e-3) / 1e6
+    result_mismatch = [int((results["batched"][s] != results["plain"][s]).sum()) for s in range(W + K)]
+    batched_vs_plain = {
+        "steps_compared": W + K, "result_mismatches": int(sum(result_mismatch)),
+        "pair_steps_compared": V, "pairs_compared": int(sum(int(p.numel()) for p in positions)),
+        "pair_mismatches": int(sum(pair_mismatch)),
+        "identical": sum(result_mismatch) == 0 and sum(pair_mismatch) == 0}
+    del saved_pairs, positions
 
     # range counts of the timed steps (for the roofline bytes), read after the timed region
-    host_res = [results[s].cpu().numpy().view(np.uint32) for s in range(W, W + K)]
+    host_res = [results["batched"][s].cpu().numpy().view(np.uint32) for s in range(W, W + K)]
     del dsteps, results
+    plans["plain"].close()
+    trees["plain"].close()
+    del plans["plain"], trees["plain"], range_out["plain"]
     torch.cuda.empty_cache()
 
     # ---- e2e: public API with pinned host buffers, CUDA graph replay, two steps in flight ----
@@ -314,7 +356,7 @@ def run_ours(args, dist: Dist):
     # range pairs run on the compute stream, and its results and packed pairs cross back on the
     # output stream once the host has its pair count, while step s + 1 runs. Buffers and plans
     # alternate between two sets.
-    e2e_steps = steps[max(W + K, Wp + Kp):]
+    e2e_steps = steps[W + K:]
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.int64 if a.dtype == np.uint64 else np.int32)).pin_memory()
     bufs = []
     for k in range(2):
@@ -326,7 +368,7 @@ def run_ours(args, dist: Dist):
             "off": torch.empty(max_ops, dtype=torch.int64, device="cuda"),
             "cap": torch.empty(max_ops, dtype=torch.int32, device="cuda"),
             "res": torch.empty(max_ops, dtype=torch.int32, device="cuda"),
-            "rout": range_out if k == 0 else torch.empty(max(1, max_pairs) * 2, dtype=torch.int32, device="cuda"),
+            "rout": range_out["batched"] if k == 0 else torch.empty(max(1, max_pairs) * 2, dtype=torch.int32, device="cuda"),
             "comp": torch.empty(max(1, max_pairs) * 2, dtype=torch.int32, device="cuda"),
             "h_res": torch.empty(max_ops, dtype=torch.int32).pin_memory(),
             "h_comp": torch.empty(max(1, max_pairs) * 2, dtype=torch.int32).pin_memory(),
@@ -355,9 +397,13 @@ def run_ours(args, dist: Dist):
             bq["h_comp"][: 2 * tot].copy_(bq["comp"][: 2 * tot], non_blocking=True)
             marks[q]["o1"].record(s_out)
             bq["ev_out"].record(s_out)
-        return b.num_ops * 4 + 8 + tot * 8
+        out_bytes_of[q] = b.num_ops * 4 + 8 + tot * 8
+        return out_bytes_of[q]
 
+    ev0, ev1 = tev(), tev()
     h2d = d2h = 0
+    in_bytes = [sum(int(h.numel() * h.element_size()) for h in hs) for hs in h_in]
+    out_bytes_of = [0] * len(e2e_steps)
     for s, b in enumerate(e2e_steps):
         bs, n = bufs[s % 2], b.num_ops
         if s == We:
@@ -387,7 +433,7 @@ def run_ours(args, dist: Dist):
         marks[s]["k1"].record(stream)
         bs["ev_k"].record(stream)
         if s >= We:
-            h2d += sum(int(h.numel() * h.element_size()) for h in h_in[s])
+            h2d += in_bytes[s]
         if s >= 1 and s != We:
             out_bytes = finish(s - 1)
             if s - 1 >= We:
@@ -400,13 +446,16 @@ def run_ours(args, dist: Dist):
     e2e_ops = sum(b.num_ops for b in e2e_steps[We:]) * dist.world
     e2e_value = e2e_ops / (e2e_ms * 1e-3) / 1e6
     e2e_stages = [{"in_ms": round(m["in0"].elapsed_time(m["in1"]), 2),
+                   "in_gbs": round(in_bytes[i] / max(1e-6, m["in0"].elapsed_time(m["in1"])) / 1e6, 1),
                    "run_ms": round(m["k0"].elapsed_time(m["k1"]), 2),
                    "out_ms": round(m["o0"].elapsed_time(m["o1"]), 2),
+                   "out_gbs": round(out_bytes_of[i] / max(1e-6, m["o0"].elapsed_time(m["o1"])) / 1e6, 1),
                    "run_start_ms": round(ev0.elapsed_time(m["k0"]), 2),
                    "gap_before_run_ms": round(marks[i - 1]["k1"].elapsed_time(m["k0"]), 2),
                    "host_run_call_ms": round(host_run[i], 2),
                    "host_wait_ms": round(host_wait[i], 2)}
                   for i, m in enumerate(marks) if i >= We]
+    copy_peak = pinned_copy_peak(torch)
 
     # ---- roofline of the persistent kernel ----
     rep = trees["batched"].validate_tree_structure()
@@ -446,29 +495,53 @@ def run_ours(args, dist: Dist):
                 rep["nodes_allocated"], rep["nodes_allocated"] * 128 / 1e9, mean_ops * 24 / 1e6),
             "tree_height": rep["height"], "workload_gen_s": round(gen_s, 1),
         },
-        "plain_per_batch": {"value": round(plain_value, 2), "unit": UNIT, "steps": Kp,
-                            "ms_per_step": round(plain_ms / Kp, 3),
-                            "batched_over_plain": round(value / plain_value, 3)},
         "e2e": {"value": round(e2e_value, 2), "unit": UNIT,
                 "h2d_bytes_per_step": int(h2d / max(1, Ke)), "d2h_bytes_per_step": int(d2h / max(1, Ke)),
                 "mode": "CUDA graph replay via the public batch API, pinned host buffers, two steps in "
                         "flight: op arrays in, results and the range pairs that exist (packed by "
                         "mvbt_batch_compact_ranges) back, overlapping the next step's run",
-                "stages": e2e_stages},
+                "stages": e2e_stages,
+                "copy_gbs": {"h2d": round(sum(in_bytes[We:]) / max(1e-6, sum(x["in_ms"] for x in e2e_stages)) / 1e6, 1),
+                             "d2h": round(sum(out_bytes_of[We:]) / max(1e-6, sum(x["out_ms"] for x in e2e_stages)) / 1e6, 1),
+                             "pinned_peak_h2d": copy_peak[0], "pinned_peak_d2h": copy_peak[1],
+                             "peak_how": "1 GiB pinned <-> device copy, best of 3, CUDA events, same process"}},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": traffic,
                      "kernel": "k_batched", "kernel_ms": round(avg_kms, 3),
                      "algorithmic_bytes_per_launch": int(avg_bytes), "peak_source": peak_kind},
         "clocks": clk,
         "gpu_launches": 5 * K,
+        "verified": {"batched_vs_plain": batched_vs_plain},
     }
+    plain = {"value": round(plain_value, 2), "unit": UNIT, "steps": K, "warmup": W,
+             "ms_per_step": round(plain_ms / K, 3), "batched_over_plain": round(value / plain_value, 3),
+             "same_steps_as_batched": True, "clocks": plain_clk,
+             "how": "the same W warm-up + K timed steps as the batched arm, on an identical tree "
+                    "(one snapshot + one mixed launch per batch)"}
+    del plans, plan, bufs, h_in, range_out
+    trees.clear()
+    torch.cuda.empty_cache()
     if args.serve_loads:
-        del plans, pplan, plan, bufs, h_in, range_out
-        trees.clear()
-        torch.cuda.empty_cache()
         out["serving"] = run_serving(args, seed, init, vals, dev)
         out["serving_p99_us"] = out["serving"]["headline"]["p99_us"]
-    return out, (init, vals, steps[W])
+    return out, plain, (init, vals, steps[0], step0)
+
+
+def pinned_copy_peak(torch, nbytes: int = 1 << 30):
+    """Best-of-3 GB/s of one pinned host -> device and one device -> pinned host copy of nbytes."""
+    h = torch.empty(nbytes, dtype=torch.uint8).pin_memory()
+    d = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+    best = [0.0, 0.0]
+    for _ in range(3):
+        for k, (dst, src) in enumerate(((d, h), (h, d))):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            dst.copy_(src, non_blocking=True)
+            b.record()
+            b.synchronize()
+            best[k] = max(best[k], nbytes / (a.elapsed_time(b) * 1e-3) / 1e9)
+    del h, d
+    return round(best[0], 1), round(best[1], 1)
 
 
 def latency_summary(arrival_ns, done_ns, ops: int) -> dict:
@@ -486,7 +559,7 @@ def run_serving(args, seed: int, init, vals, dev) -> dict:
     Latency = arrival to results on the host; throughput = ops / (start to last completion)."""
     import torch
     import mvgpubtree_b200 as mv
-    from mvgpubtree_b200 import workload as wl
+    import workload as wl
     loads = [float(x) for x in str(args.serve_loads).split(",") if x.strip()]
     pool = int(args.pool_gb * (1 << 30))
     trees = {"batched": mv.gpu_versioned_btree(pool_bytes=pool, tile_width=args.tile_width, reclaim=True),
@@ -529,38 +602,6 @@ def run_serving(args, seed: int, init, vals, dev) -> dict:
 # ------------------------------------------------------------------------------------------------
 # CPU side: the oracle (the reference-side CPU implementation of the path), timed on host cores
 # ------------------------------------------------------------------------------------------------
-def _sample(b, max_ops: int):
-    """The first batches of step b holding at most max_ops ops (at least one batch)."""
-    from mvgpubtree_b200.workload import Batches
-    nb = 1
-    while nb < b.num_batches and int(b.batch_off[nb + 1]) <= max_ops:
-        nb += 1
-    end = int(b.batch_off[nb])
-    r = b.type[:end] == 3
-    return Batches(b.batch_off[: nb + 1].copy(), b.type[:end], b.key[:end], b.arg[:end],
-                   b.out_off[:end], b.range_cap[:end],
-                   int((b.out_off[:end][r] + b.range_cap[:end][r]).max()) if r.any() else 0)
-
-
-def cpu_oracle_time(init, vals, batches, max_ops: int):
-    """Builds the partitioned oracle (untimed) and times its run of each sampled batch list."""
-    import oracle
-    cores = os.cpu_count() or 1
-    m = oracle.PartitionedMVMap(cores, versioned=True)
-    t0 = time.time()
-    m.insert(init, vals)
-    build_s = time.time() - t0
-    times, ops = [], []
-    for b in batches:
-        s = _sample(b, max_ops)
-        t0 = time.perf_counter()
-        m.run_batches(s, with_pairs=True)
-        times.append(time.perf_counter() - t0)
-        ops.append(s.num_ops)
-    m.close()
-    return cores, build_s, times, ops
-
-
 REF_DRIVER = Path(__file__).resolve().parent / "oracle" / "_ref" / "ref_driver"
 
 # ------------------------------------------------------------------------------------------------
@@ -603,11 +644,13 @@ def _hmean(xs):
 
 def run_configs_ours(args) -> dict:
     """Configs 1-3 through this library's reference-named host API, tile widths 8 and 16 (the
-    faster is reported). Results are checked where a full-size check is cheap: every c1 and c2 find
-    against the value function of its key."""
+    faster is reported). Every result is checked against the oracle at full size: each c1 and c2
+    find, and each c3 range count and range pair (all 9 mixes, 40M keys, 10M ops) at the snapshot
+    taken before the inserts (oracle.SortedSnapshot of the initial keys)."""
     import torch
     import mvgpubtree_b200 as mv
-    from mvgpubtree_b200 import workload as wl
+    import oracle
+    import workload as wl
 
     seed, reps = args.seed, max(1, args.config_reps)
     stream = torch.cuda.current_stream()
@@ -641,7 +684,7 @@ def run_configs_ours(args) -> dict:
     keys = wl.distinct_keys(seed, 0, n)
     vals = wl.values_for(keys, seed)
     q = hit_miss_queries(wl, seed, keys)
-    expect = np.where(np.isin(q, keys, assume_unique=True), wl.values_for(q, seed), 0xFFFFFFFF).astype(np.uint32)
+    expect = oracle.SortedSnapshot(keys, vals).find(q)
     dk, dv, dq = dev(keys), dev(vals), dev(q)
     r0 = torch.empty(n, dtype=torch.int32, device="cuda")
     best = None
@@ -661,9 +704,12 @@ def run_configs_ours(args) -> dict:
     keys = wl.distinct_keys(seed, 0, n)
     upd = wl.shuffle(seed + 3, keys)[:u]
     q = hit_miss_queries(wl, seed, keys)
-    hit = np.isin(q, keys, assume_unique=True)
-    e0 = np.where(hit, wl.values_for(q, seed), 0xFFFFFFFF).astype(np.uint32)
-    e1 = np.where(np.isin(q, upd, assume_unique=True), wl.values_for(q, seed ^ 1), e0).astype(np.uint32)
+    v0 = wl.values_for(keys, seed)
+    e0 = oracle.SortedSnapshot(keys, v0).find(q)
+    v1 = v0.copy()
+    v1[np.isin(keys, upd, assume_unique=True)] = wl.values_for(keys[np.isin(keys, upd, assume_unique=True)], seed ^ 1)
+    e1 = oracle.SortedSnapshot(keys, v1).find(q)
+    del v0, v1
     dk, dv, du, duv, dq = dev(keys), dev(wl.values_for(keys, seed)), dev(upd), dev(wl.values_for(upd, seed ^ 1)), dev(q)
     r0 = torch.empty(n, dtype=torch.int32, device="cuda")
     r1 = torch.empty(n, dtype=torch.int32, device="cuda")
@@ -691,7 +737,12 @@ def run_configs_ours(args) -> dict:
     N = args.initial_keys
     stride = wl.stride_for(N)
     keys = wl.distinct_keys(seed, 0, N)
-    dk, dv = dev(keys), dev(wl.values_for(keys, seed))
+    kvals = wl.values_for(keys, seed)
+    dk, dv = dev(keys), dev(kvals)
+    # the oracle's state at the snapshot every c3 range query reads: the initial keys
+    snap = oracle.SortedSnapshot(keys, kvals)
+    d_sk, d_sv = dev(snap.keys), dev(snap.values)
+    del kvals
     base, insert_mops = {}, {}
     for w in (8, 16):
         ms = []
@@ -705,10 +756,18 @@ def run_configs_ours(args) -> dict:
     del dk, dv
     runs = {8: {}, 16: {}}
     seq = {8: {}, 16: {}}
+    checks = {}
+    lo_start = (None, None)
     for u, L, n_ins, n_rq in c3_combos(seed):
         ins = wl.distinct_keys(seed, N, n_ins)
         lo = wl.uniform_keys(seed + 1, n_rq)
-        di, div, dlo, dhi = dev(ins), dev(wl.values_for(ins, seed)), dev(lo), dev(wl.upper_bounds(lo, L, stride))
+        hi = wl.upper_bounds(lo, L, stride)
+        if lo_start[0] != n_rq:  # the lower bounds of a given u are shared by its three lengths
+            lo_start = (n_rq, snap.lower_bound(lo))
+        a = lo_start[1]
+        c = np.maximum(snap.lower_bound(hi) - a, 0)
+        d_a, d_c = torch.from_numpy(a).cuda(), torch.from_numpy(c).cuda()
+        di, div, dlo, dhi = dev(ins), dev(wl.values_for(ins, seed)), dev(lo), dev(hi)
         pairs = torch.empty(n_rq * 2 * L * 2, dtype=torch.int32, device="cuda")
         counts = torch.empty(n_rq, dtype=torch.int32, device="cuda")
         name = f"u{int(u * 100)}_L{L}"
@@ -717,24 +776,63 @@ def run_configs_ours(args) -> dict:
             s = t.take_snapshot()
             return [timed(lambda: (t.insert(di, div), t.range_query(dlo, dhi, pairs, counts, 2 * L, n_rq, s)))]
 
+        chk = {"queries": n_rq, "pairs": int(np.minimum(c, 2 * L).sum()), "max_count": int(c.max()) if n_rq else 0}
         for w in (8, 16):
             ms = mean_runs(lambda: base[w].clone(),
                            lambda t: [timed(lambda: t.concurrent_insert_range(
-                               di, div, n_ins, dlo, dhi, n_rq, pairs, 2 * L))])
+                               di, div, n_ins, dlo, dhi, n_rq, pairs, 2 * L, counts))])
             runs[w][name] = round(C3_OPS / ms[0] / 1e3, 1)
+            chk[f"w{w}_concurrent_bad"] = check_ranges_device(torch, counts, pairs, d_a, d_c, 2 * L, d_sk, d_sv)
             ms = mean_runs(lambda: base[w].clone(), sequence)
             seq[w][name] = round(C3_OPS / ms[0] / 1e3, 1)
-        del di, div, dlo, dhi, pairs, counts
+            chk[f"w{w}_sequence_bad"] = check_ranges_device(torch, counts, pairs, d_a, d_c, 2 * L, d_sk, d_sv)
+        checks[name] = chk
+        del di, div, dlo, dhi, pairs, counts, d_a, d_c
         torch.cuda.empty_cache()
     for t in base.values():
         t.close()
+    del d_sk, d_sv
     w = max(runs, key=lambda k: _hmean(list(runs[k].values())))
+    wi = max(insert_mops, key=insert_mops.get)
+    bad = sum(sum(x for k, v in ch.items() if k.endswith("_bad") for x in v) for ch in checks.values())
     out["c3_insert_range_40M"] = {
-        "tile_width": w, "insert_40M_mops": insert_mops[w],
+        "tile_width": w, "insert_40M_mops": insert_mops[wi], "insert_tile_width": wi,
+        "insert_40M_mops_by_width": insert_mops,
         "concurrent_mops": runs[w], "concurrent_hmean_mops": round(_hmean(list(runs[w].values())), 1),
-        "sequence_mops": seq[w], "sequence_hmean_mops": round(_hmean(list(seq[w].values())), 1)}
+        "sequence_mops": seq[w], "sequence_hmean_mops": round(_hmean(list(seq[w].values())), 1),
+        "verified": bad == 0,
+        "check": {"how": "every range count and every pair min(count, 2L) of every query, both tile "
+                         "widths, concurrent and sequence forms, against the oracle's state at the "
+                         "launch snapshot (the initial 40M keys)",
+                  "per_mix": checks}}
     torch.cuda.empty_cache()
     return out
+
+
+def check_ranges_device(torch, counts, pairs, d_start, d_count, cap, d_keys, d_values, chunk=1 << 18):
+    """[count mismatches, pair mismatches] of range results against the oracle's answer: query i
+    holds d_count[i] hits, the keys d_keys[d_start[i] : d_start[i] + d_count[i]] (sorted snapshot
+    arrays from oracle.SortedSnapshot, shipped to the device) with their values; its first
+    min(count, cap) pairs sit at pairs[i * cap ...]. The comparison gathers on the device, so the
+    tens of GB of fixed-size slots never cross to the host."""
+    got = counts.long() & 0xFFFFFFFF
+    bad_counts = int((got != d_count).sum())
+    P = pairs.view(-1, 2)
+    bad_pairs = 0
+    n = int(d_count.numel())
+    for q0 in range(0, n, chunk):
+        q1 = min(n, q0 + chunk)
+        take = torch.clamp(d_count[q0:q1], max=cap)
+        total = int(take.sum())
+        if total == 0:
+            continue
+        starts = torch.cumsum(take, 0) - take
+        j = torch.arange(total, device=take.device) - torch.repeat_interleave(starts, take)
+        qi = torch.repeat_interleave(torch.arange(q0, q1, device=take.device), take)
+        g = P[qi * cap + j]
+        e = d_start[qi] + j
+        bad_pairs += int(((g[:, 0] != d_keys[e]) | (g[:, 1] != d_values[e])).sum())
+    return [bad_counts, bad_pairs]
 
 
 def run_configs_reference(args) -> dict:
@@ -791,44 +889,109 @@ def reference_build_time(args, W: int, K: int):
 
 
 def run_reference(args, dist: Dist):
-    """Reference arm (rank 0 only): the reference implementation's own CUDA build on this B200 and
-    this workload; the oracle port on the host cores is reported beside it as cpu_baseline (and is
-    the arm's value where the reference build is absent)."""
+    """Reference arm (rank 0 only): the reference implementation's own CUDA build
+    (oracle/_ref/ref_driver, from its unmodified headers) on this B200 and this workload, through
+    its public host API. The oracle port on the host cores (one full step) is reported beside it as
+    cpu_baseline. Without a reference build the arm reports value null with the reason. This
+    process loads no library of this repository's product: the workload generator is the host-only
+    workload/libworkload.so and the CPU map is oracle/liboracle.so."""
     if dist.rank != 0:
         return None
     W, K = max(3, args.warmup), args.steps
     configs = None if args.no_configs else run_configs_reference(args)
     ref, why = reference_build_time(args, W, K)
-    init, vals, steps, _ = make_workload(args.seed, args.initial_keys, W + K, args.batches)
-    cores, build_s, times, ops = cpu_oracle_time(init, vals, steps, args.cpu_sample_ops)
-    t = sum(times[W:])
-    n = sum(ops[W:])
-    cpu_value = n / t / 1e6
-    sample = (f"first batches of each step up to {args.cpu_sample_ops} ops (mean "
-              f"{int(n / K)} ops/step) on the 40M-key map; build {build_s:.1f} s untimed")
-    cpu = {"value": round(cpu_value, 3), "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
+    init, vals, steps, _ = make_workload(args.seed, args.initial_keys, 1, args.batches)
+    cpu = None
+    if not args.no_cpu_baseline:
+        import oracle
+        cores = os.cpu_count() or 1
+        m = oracle.PartitionedMVMap(cores, versioned=True)
+        t0 = time.time()
+        m.insert(init, vals)
+        build_s = time.time() - t0
+        t0 = time.perf_counter()
+        m.run_batches(steps[0], with_pairs=True)
+        run_s = time.perf_counter() - t0
+        m.close()
+        cpu = {"value": round(steps[0].num_ops / run_s / 1e6, 3), "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": f"one full step ({steps[0].num_ops} ops in {steps[0].num_batches} batches) on the "
+                         f"40M-key oracle map, {cores} threads; build {build_s:.1f} s untimed"}
     config = {"workload": "mixed batches on a 40M-key versioned tree, one snapshot per batch "
                           "(same generator, seed and batches as the GPU arm)",
-              "initial_keys": args.initial_keys, "batches_per_step": args.batches}
-    if ref is not None:
-        value, ms_per_step = ref["mops"], ref["ms"] / K
-        config["implementation"] = ("reference CUDA build (unmodified headers, nvcc sm_100a, its own "
-                                    "flags) through its public host API, one batch at a time: "
-                                    "take_snapshot, find(ts), range_query(ts), insert(in_place), erase")
-        config["ops_timed"] = ref["ops_timed"]
+              "initial_keys": args.initial_keys, "batches_per_step": args.batches,
+              "implementation": "reference CUDA build (unmodified headers, nvcc sm_100a, its own "
+                                "flags) through its public host API, one batch at a time: "
+                                "take_snapshot, find(ts), range_query(ts), insert(in_place), erase; "
+                                "op arrays resident on the device"}
+    line = {"impl": "reference", "metric": METRIC, "unit": UNIT, "n_gpus": dist.world, "steps": K,
+            "warmup": W, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic (seeded)", "config": config}
+    if ref is None:
+        line.update({"value": None, "unavailable": why})
     else:
-        value, ms_per_step = cpu_value, 1e3 * t / K
-        config["implementation"] = ("oracle multiversion ordered map (std::map per key-range partition, "
-                                    f"one partition per host thread); {why}")
-    return {
-        "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": UNIT,
-        "n_gpus": dist.world, "steps": K, "warmup": W, "ms_per_step": round(ms_per_step, 3),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
-        "data": "synthetic (seeded)", "config": config,
-        "cpu_baseline": cpu,
-        "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        **({"configs": configs} if configs is not None else {}),
-    }
+        value = round(ref["mops"], 3)
+        config["ops_timed"] = ref["ops_timed"]
+        line.update({"value": value, "ms_per_step": round(ref["ms"] / K, 3),
+                     "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
+    if configs is not None:
+        line["configs"] = configs
+    return line
+
+
+def oracle_step_check(init, vals, b, gpu_result, gpu_pairs):
+    """One full step of mixed batches on the partitioned oracle (all host cores; the map is built
+    from the initial keys, untimed): its run is timed (the CPU baseline) and every result -- find
+    value, range count, and each of the first min(count, cap) pairs of every range query -- is
+    compared with the GPU's results of the same step on the same initial tree."""
+    import oracle
+    cores = os.cpu_count() or 1
+    m = oracle.PartitionedMVMap(cores, versioned=True)
+    t0 = time.time()
+    m.insert(init, vals)
+    build_s = time.time() - t0
+    t0 = time.perf_counter()
+    res, out = m.run_batches(b, with_pairs=True)
+    run_s = time.perf_counter() - t0
+    m.close()
+    r = b.type == 3
+    take = np.minimum(res[r], b.range_cap[r]).astype(np.int64)
+    pos = np.repeat(b.out_off[r].astype(np.int64) - (np.cumsum(take) - take), take) + np.arange(int(take.sum()))
+    exp_pairs = out.reshape(-1, 2)[pos]
+    got_pairs = gpu_pairs[pos]
+    bad_res = int(np.count_nonzero(res != gpu_result))
+    bad_pairs = int(np.count_nonzero((exp_pairs != got_pairs).any(axis=1)))
+    check = {"ops": int(b.num_ops), "results_compared": int(res.size), "result_mismatches": bad_res,
+             "pairs_compared": int(pos.size), "pair_mismatches": bad_pairs,
+             "identical": bad_res == 0 and bad_pairs == 0,
+             "how": "step 0 (256 batches) of the bench workload from the initial 40M-key tree, GPU "
+                    "(persistent launch) against the partitioned multiversion-map oracle"}
+    cpu = {"value": round(b.num_ops / run_s / 1e6, 3), "unit": UNIT, "cores": cores, "kind": "port",
+           "sample": f"one full step ({b.num_ops} ops in {b.num_batches} batches) on the 40M-key oracle "
+                     f"map, {cores} threads; build {build_s:.1f} s untimed"}
+    return check, cpu
+
+
+def reference_step_check(args, seed: int, b, gpu_result, gpu_pairs) -> dict:
+    """Checksums of every result of step 0 from the reference implementation's own CUDA build
+    (oracle/_ref/ref_driver, same generator, seed and initial tree, each batch through its public
+    host API) against the same sums of this library's step 0 (oracle/refsums.py)."""
+    from oracle import refsums
+    if not REF_DRIVER.exists():
+        return {"unavailable": "reference build not present"}
+    try:
+        ref = refsums.run_driver("c4", "--initial", str(args.initial_keys), "--batches", str(args.batches),
+                                 "--steps", "1", "--warmup", "0", "--seed", str(seed), "--checksums", "1",
+                                 timeout=900)
+    except (RuntimeError, subprocess.TimeoutExpired) as e:
+        return {"unavailable": str(e)[-300:]}
+    ours = refsums.step_sums(b, gpu_result, gpu_pairs)
+    theirs = [int(x) for x in ref["step_checksums"][0]]
+    return {"identical": ours == theirs, "ours": [str(x) for x in ours], "reference": [str(x) for x in theirs],
+            "how": "find / range-count / range-pair checksums of step 0 (256 batches, same seed) from "
+                   "the reference's CUDA build (take_snapshot, find(ts), range_query(ts), insert, erase "
+                   "per batch) and from this library's persistent launch"}
 
 
 def main():
@@ -842,16 +1005,22 @@ def main():
     configs = None
     if dist.world == 1 and not args.no_configs:
         configs = run_configs_ours(args)
-    out, cpu_inputs = run_ours(args, dist)
+    out, plain, (init, vals, b0, step0) = run_ours(args, dist)
+    if dist.rank == 0 and dist.world == 1:
+        res0, pairs0 = step0
+        if not args.no_cpu_baseline:
+            check, cpu = oracle_step_check(init, vals, b0, res0, pairs0)
+            out["verified"]["c4_step0_vs_oracle"] = check
+            out["cpu_baseline"] = cpu
+        out["verified"]["c4_step0_vs_reference_build"] = reference_step_check(args, args.seed, b0, res0, pairs0)
+    v = out["verified"]
+    out["verified"]["all"] = bool(v["batched_vs_plain"]["identical"]
+                                  and v.get("c4_step0_vs_oracle", {}).get("identical", False)
+                                  and all(c.get("verified", False) for c in (configs or {}).values()))
+    # the comparison with the plain per-batch launch and the other configs go last on the line
     if configs is not None:
         out["configs"] = configs
-    if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
-        init, vals, step = cpu_inputs
-        cores, build_s, times, ops = cpu_oracle_time(init, vals, [step], args.cpu_sample_ops)
-        out["cpu_baseline"] = {
-            "value": round(ops[0] / times[0] / 1e6, 3), "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"{ops[0]} ops (first batches of one step) on the 40M-key oracle map, "
-                      f"{cores} threads; build {build_s:.1f} s untimed"}
+    out["plain_per_batch"] = plain
     if dist.rank == 0:
         print(json.dumps(out), flush=True)
     dist.close()

@@ -218,9 +218,10 @@ int mvbt_reclaim(mvbt_tree* tree, uint32_t min_live_snapshot, void* stream);
 
 /* Device counters (synchronises the device): out[0] versions copied, [1] node splits, [2] longest
  * locked move-right walk, [3] longest unlocked writer descent, [4] write epoch, [5] error bits,
- * [6..21] errors per raising site, [22] locked approaches restarted unlocked, [23] nodes freed by
- * mvbt_reclaim, [24] freed nodes waiting for reuse, [25] nodes handed out again, [26] copies the
- * full retire log could not record (never freed). Writes min(n, 27) values. */
+ * [6..21] errors per raising site 0..15, [22] locked approaches restarted unlocked, [23] nodes
+ * freed by mvbt_reclaim, [24] freed nodes waiting for reuse, [25] nodes handed out again, [26]
+ * copies the full retire log could not record (never freed), [27..42] errors per raising site
+ * 16..31 (16: rejected batch offsets of mvbt_batch_run_noalloc). Writes min(n, 43) values. */
 int mvbt_stats(mvbt_tree* tree, uint64_t* out, uint32_t n);
 
 /* Device view for user kernels calling the cooperative_* device API. */
@@ -322,8 +323,8 @@ int mvbt_batch_run_noalloc(mvbt_tree* tree, uint32_t num_batches, const uint64_t
  * pipeline_depth launches staged or running; copies overlap compute on two more streams).
  * Between launches a reclaim pass frees the version copies the finished snapshots read
  * (config.reclaim trees). Results and completion times come back per request. Requests of one
- * group must not write the same key (a trace from mvbt_wl_mix_* with erase_lag above
- * max_requests_per_launch guarantees it). It has no counterpart in the reference, which has no
+ * group must not write the same key (a trace from the workload generator,
+ * workload/mvbt_workload.h, with erase_lag above max_requests_per_launch guarantees it). It has no counterpart in the reference, which has no
  * serving path. */
 #define MVBT_SERVE_SNAPSHOT_PER_BATCH 0u
 #define MVBT_SERVE_SNAPSHOT_PER_REQUEST 1u
@@ -361,7 +362,8 @@ void mvbt_serve_config_init(mvbt_serve_config* cfg);
  * Request r holds ops [req_off[r], req_off[r + 1]) of type/key/arg/range_cap (as in
  * mvbt_batch_run) and arrives arrival_ns[r] after the session start (non-decreasing). Range
  * query i writes at most range_cap[i] pairs at range_out + out_off[i]; the slots of all range
- * queries must be disjoint and increasing in op order (as mvbt_wl_mix_copy produces them).
+ * queries must be disjoint and increasing in op order (as the workload generator's
+ * mvbt_wl_mix_copy produces them).
  * Outputs: result[i] per op, the range pairs (a query's slot past its count, and any gap between
  * slots, is unspecified), done_ns[r] (session clock when the request's results were on the host),
  * snapshot[r] (the snapshot its reads used: requests with the same one formed one group; may be

@@ -178,7 +178,8 @@ struct control_block {
   unsigned long long stat_max_hops;   // longest move-right walk under locks
   unsigned long long stat_max_steps;  // longest unlocked descent of a writer (node visits)
   unsigned long long stat_restarts;   // locked approaches abandoned for an unlocked re-approach
-  uint32_t err_site[16];              // errors per raising site (diagnostics)
+  uint32_t err_site[32];              // errors per raising site (diagnostics; 16 = the
+                                      // offsets check of mvbt_batch_run_noalloc)
   unsigned long long sm_pool[kMaxSmSlots];  // per-SM chunk cursor: (base << 32) | used
   // Reclamation of version copies (off when reclaim_cap == 0). The retire log holds the index of
   // every copy made since the last reclaim pass, the free ring the nodes a pass freed; allocation
@@ -255,7 +256,7 @@ MVBT_HD void init_control(control_block& c, uint32_t capacity, uint32_t chunk, u
   c.stat_max_hops  = 0;
   c.stat_restarts  = 0;
   c.stat_max_steps = 0;
-  for (int i = 0; i < 16; ++i) c.err_site[i] = 0;
+  for (int i = 0; i < 32; ++i) c.err_site[i] = 0;
   // used == chunk: the first allocation on each SM refills its chunk from the bump pointer
   for (int i = 0; i < kMaxSmSlots; ++i) c.sm_pool[i] = chunk;
   for (int i = 0; i < kMaxSmSlots; ++i)
@@ -692,7 +693,7 @@ struct device_tree {
 
   MVBT_DEV void set_error(uint32_t bits, uint32_t site = 0) const {
     atomicOr(&ctl->error, bits);
-    atomicAdd(&ctl->err_site[site & 15], 1u);
+    atomicAdd(&ctl->err_site[site & 31], 1u);
   }
   MVBT_DEV uint32_t current_epoch() const { return ld_relaxed_u32(&ctl->epoch); }
 

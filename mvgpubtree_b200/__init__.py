@@ -134,15 +134,29 @@ def _check(status: int, where: str) -> None:
         raise MVBTError(status, where)
 
 
+PAIRS = 0  # word_bytes of a pair buffer: {key, value} uint32 pairs held in 4- or 8-byte elements
+
+
 def _ptr(x, word_bytes: int = 4, name: str = "array"):
-    """Device address of a CUDA tensor, a pinned host tensor or a raw pointer (int)."""
+    """Device address of a CUDA tensor, a pinned host tensor or a raw pointer (int).
+
+    word_bytes is the element size the C ABI reads through the pointer: 4 for uint32 arrays, 8 for
+    uint64 arrays (offsets, totals; an integer dtype is required), PAIRS for pair buffers. A tensor
+    of another element size is rejected: the kernels would read it with the wrong stride, past
+    its end."""
     if x is None:
         return None
     if isinstance(x, int):
         return x
     if hasattr(x, "data_ptr"):
-        if x.element_size() not in (4, 8):
-            raise TypeError(f"{name}: expected 32- or 64-bit elements, got {x.element_size()} bytes")
+        es = x.element_size()
+        if word_bytes == PAIRS:
+            if es not in (4, 8):
+                raise TypeError(f"{name}: a pair buffer needs 32- or 64-bit elements, got {es} bytes")
+        elif es != word_bytes:
+            raise TypeError(f"{name}: expected {8 * word_bytes}-bit elements, got {8 * es}-bit ones")
+        if word_bytes == 8 and (x.is_floating_point() or x.is_complex()):
+            raise TypeError(f"{name}: expected an integer dtype, got {x.dtype}")
         if not x.is_contiguous():
             raise ValueError(f"{name} must be contiguous")
         if not x.is_cuda and not x.is_pinned():
@@ -273,7 +287,7 @@ class _TreeBase:
                     concurrent: bool = False):
         n = _numel(lower_bound) if num_keys is None else int(num_keys)
         _check(lib.mvbt_range_query(self._h, _ptr(lower_bound, name="lower"), _ptr(upper_bound, name="upper"),
-                                    _ptr(result, 8, "result"), _ptr(counts, name="counts"),
+                                    _ptr(result, PAIRS, "result"), _ptr(counts, name="counts"),
                                     int(average_range_length), n, int(timestamp), _stream(stream),
                                     int(bool(concurrent))), "range_query")
 
@@ -283,7 +297,7 @@ class _TreeBase:
         _check(lib.mvbt_concurrent_insert_range(
             self._h, _ptr(keys, name="keys"), _ptr(values, name="values"), int(num_insertion),
             _ptr(lower_bound, name="lower"), _ptr(upper_bound, name="upper"), int(num_ranges),
-            _ptr(result, 8, "result"), int(average_range_length), _ptr(counts, name="counts"),
+            _ptr(result, PAIRS, "result"), int(average_range_length), _ptr(counts, name="counts"),
             _stream(stream)), "concurrent_insert_range")
 
     def concurrent_find_erase(self, find_keys, find_results, num_finds: int, erase_keys,
@@ -339,11 +353,12 @@ class _TreeBase:
 
     def stats(self) -> dict:
         """Device counters: versions copied, splits, longest walks, epoch, error bits per site."""
-        buf = (_u64 * 27)()
-        _check(lib.mvbt_stats(self._h, buf, 27), "stats")
+        buf = (_u64 * 43)()
+        _check(lib.mvbt_stats(self._h, buf, 43), "stats")
         v = list(buf)
+        sites = v[6:22] + v[27:43]
         return {"cow": v[0], "splits": v[1], "max_hops": v[2], "max_descent": v[3], "epoch": v[4],
-                "error_bits": v[5], "error_sites": {i: v[6 + i] for i in range(16) if v[6 + i]},
+                "error_bits": v[5], "error_sites": {i: x for i, x in enumerate(sites) if x},
                 "restarts": v[22], "reclaimed": v[23], "free_nodes": v[24], "reused": v[25],
                 "log_dropped": v[26]}
 
@@ -394,12 +409,12 @@ class gpu_versioned_btree(_TreeBase):
             self._h, int(batch_off.numel()) - 1, _ptr(batch_off, 8, "batch_off"), int(num_ops),
             _ptr(type, name="type"), _ptr(key, name="key"), _ptr(arg, name="arg"),
             _ptr(out_off, 8, "out_off"), _ptr(range_cap, name="range_cap"),
-            _ptr(result, name="result"), _ptr(range_out, 8, "range_out"), _stream(stream)),
+            _ptr(result, name="result"), _ptr(range_out, PAIRS, "range_out"), _stream(stream)),
             "batch_run_noalloc")
 
     def serve(self, batches, arrival_ns, **config) -> dict:
         """Serving session over a trace (mvbt_serve_trace): request r is batch r of `batches`
-        (mvgpubtree_b200.workload.Batches, generated in one call so range slots increase) and
+        (workload.Batches, generated in one call so range slots increase) and
         arrives arrival_ns[r] after the session start. Config keys are the mvbt_serve_config
         fields (mode, snapshots: SERVE_SNAPSHOT_PER_BATCH or _PER_REQUEST, pipeline_depth,
         max_ops_per_launch, max_requests_per_launch, max_range_pairs, reclaim_every,
@@ -489,7 +504,7 @@ class BatchPlan:
         _check(lib.mvbt_batch_run(self._h, len(off) - 1, off.ctypes.data, _ptr(type, name="type"),
                                   _ptr(key, name="key"), _ptr(arg, name="arg"),
                                   _ptr(out_off, 8, "out_off"), _ptr(range_cap, name="range_cap"),
-                                  _ptr(result, name="result"), _ptr(range_out, 8, "range_out"),
+                                  _ptr(result, name="result"), _ptr(range_out, PAIRS, "range_out"),
                                   int(mode), _stream(stream)), "batch_run")
 
     def compact_ranges(self, num_ops: int, type, result, out_off, range_cap, range_out, compact, total,
@@ -500,8 +515,8 @@ class BatchPlan:
         over the range queries before it."""
         _check(lib.mvbt_batch_compact_ranges(self._h, int(num_ops), _ptr(type, name="type"),
                                              _ptr(result, name="result"), _ptr(out_off, 8, "out_off"),
-                                             _ptr(range_cap, name="range_cap"), _ptr(range_out, 8, "range_out"),
-                                             _ptr(compact, 8, "compact"), _ptr(total, 8, "total"),
+                                             _ptr(range_cap, name="range_cap"), _ptr(range_out, PAIRS, "range_out"),
+                                             _ptr(compact, PAIRS, "compact"), _ptr(total, 8, "total"),
                                              _stream(stream)), "compact_ranges")
 
     def set_launch(self, tile_width: int = 0, blocks_per_sm: int = -1) -> None:

@@ -614,7 +614,7 @@ __global__ void k_noalloc_setup(const uint64_t* __restrict__ caller_off, uint32_
     params[1] = 0;
     if (!ok) {
       atomicOr(&ctl->error, mvbt::kErrCorrupt);
-      atomicAdd(&ctl->err_site[13], 1u);
+      atomicAdd(&ctl->err_site[16], 1u);  // its own site: the offsets check of this entry point
     }
   }
 }

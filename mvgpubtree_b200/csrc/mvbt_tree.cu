@@ -949,7 +949,7 @@ int mvbt_stats(mvbt_tree* t, uint64_t* out, uint32_t n) {
   control_block c;
   MVBT_CUDA_TRY(cudaMemcpy(&c, t->ctl, sizeof(c), cudaMemcpyDeviceToHost));
   const bool rc  = c.reclaim_cap != 0;
-  uint64_t v[27] = {rc ? c.retire_tail : mvbt::stat_total(c, 0), mvbt::stat_total(c, 1), c.stat_max_hops,
+  uint64_t v[43] = {rc ? c.retire_tail : mvbt::stat_total(c, 0), mvbt::stat_total(c, 1), c.stat_max_hops,
                     c.stat_max_steps,
                     c.epoch, c.error};
   for (int i = 0; i < 16; ++i) v[6 + i] = c.err_site[i];
@@ -959,7 +959,8 @@ int mvbt_stats(mvbt_tree* t, uint64_t* out, uint32_t n) {
   v[24] = rc ? c.free_tail - fh : 0;
   v[25] = c.stat_reused + (rc ? fh - c.free_mark : 0);
   v[26] = c.stat_log_dropped;
-  for (uint32_t i = 0; i < n && i < 27; ++i) out[i] = v[i];
+  for (int i = 0; i < 16; ++i) v[27 + i] = c.err_site[16 + i];
+  for (uint32_t i = 0; i < n && i < 43; ++i) out[i] = v[i];
   return MVBT_OK;
 }
 

@@ -115,7 +115,7 @@ class MVMap:
         return k, v
 
     def run_batches(self, b, with_pairs: bool = True):
-        """Applies mixed batches (mvgpubtree_b200.workload.Batches); returns (result, range_out)."""
+        """Applies mixed batches (workload.Batches); returns (result, range_out)."""
         result = np.zeros(b.num_ops, np.uint32)
         out = np.full(max(1, b.range_pairs) * 2, 0xFFFFFFFF, np.uint32) if with_pairs else None
         self._lib.orc_run_batches(self._h, b.num_batches, b.batch_off, b.type, b.key, b.arg,
@@ -151,3 +151,41 @@ class PartitionedMVMap:
                                        b.out_off, b.range_cap, result,
                                        out.ctypes.data if with_pairs else None)
         return result, out
+
+
+class SortedSnapshot:
+    """The oracle's state at one snapshot of a tree that holds exactly `keys` -> `values` (plus the
+    tombstone key 0 -> 0 every tree starts with), as sorted arrays. Range queries follow the
+    reference's validator (include/validation.hpp:205-238: std::set::lower_bound, then walk while
+    key < upper): the hits of [lo, hi) are the keys at sorted positions [lower_bound(lo),
+    lower_bound(hi)), ascending. Used where the state is a plain key set (the initial tree of a
+    workload) and the queries are too many for the ordered-map oracle's walk: needles are sorted
+    before the binary searches, which keeps them cache-friendly."""
+
+    def __init__(self, keys, values):
+        k = np.concatenate([np.zeros(1, np.uint32), _u32(keys)])
+        v = np.concatenate([np.zeros(1, np.uint32), _u32(values)])
+        order = np.argsort(k, kind="stable")
+        self.keys, self.values = k[order], v[order]
+        if self.keys.size > 1 and not np.all(self.keys[1:] > self.keys[:-1]):
+            raise ValueError("SortedSnapshot needs distinct keys")
+
+    def lower_bound(self, q) -> np.ndarray:
+        q = _u32(q)
+        order = np.argsort(q, kind="stable")
+        out = np.empty(q.size, np.int64)
+        out[order] = np.searchsorted(self.keys, q[order], side="left")
+        return out
+
+    def range_query(self, lower, upper):
+        """(start, count): query i's hits are keys[start[i] : start[i] + count[i]] (an empty range
+        when upper <= lower, as in validation.hpp)."""
+        a = self.lower_bound(lower)
+        b = self.lower_bound(upper)
+        return a, np.maximum(b - a, 0)
+
+    def find(self, q) -> np.ndarray:
+        q = _u32(q)
+        pos = np.minimum(self.lower_bound(q), self.keys.size - 1)
+        hit = self.keys[pos] == q
+        return np.where(hit, self.values[pos], np.uint32(NOT_FOUND)).astype(np.uint32)

@@ -1,6 +1,6 @@
 // ref_driver.cu -- runs the reference implementation (owensgroup/MVGpuBTree, its unmodified
 // headers) through the reference's own public host API, on workloads from this repository's
-// generator (include/mvbt_workload.h), and prints one JSON line with throughput and checksums of
+// generator (workload/mvbt_workload.h), and prints one JSON line with throughput and checksums of
 // every result. It is test and baseline infrastructure: oracle/ref_build.py compiles it, and only
 // the tests and bench.py's reference arm run it.
 //
@@ -50,7 +50,7 @@
 #include <string>
 #include <vector>
 
-#include "../include/mvbt_workload.h"
+#include "../workload/mvbt_workload.h"
 
 namespace {
 
@@ -58,13 +58,27 @@ using key_t   = uint32_t;
 using value_t = uint32_t;
 using pair_t  = pair_type<key_t, value_t>;
 using vnode_t = GpuBTree::node_type<key_t, value_t, 16>;
-// 2^28 nodes (32 GiB): room for a 40M-key tree and the versions of many steps of batches. The
-// reference's bump allocator does not check its bound (include/device_bump_allocator.hpp:46-54),
-// so the driver refuses workloads that could come near it (kPoolNodes).
-using valloc_t  = device_bump_allocator<vnode_t, (1ull << 28)>;
+// 2^29 nodes (64 GiB of the B200's 180 GB): room for a 40M-key tree and the versions of 25 steps
+// of 256 mixed batches (about 180M nodes by the estimate below; the reference's tree measured
+// about 1 node per write). The reference's bump allocator does not check its bound
+// (include/device_bump_allocator.hpp:46-54), so the driver refuses workloads whose estimate could
+// come near it (pool_estimate_ok) and reads the allocator's count between steps (untimed), stopping
+// with an error before a step could reach the bound.
+using valloc_t  = device_bump_allocator<vnode_t, (1ull << 29)>;
 using vtree_t   = GpuBTree::gpu_versioned_btree<key_t, value_t, 16, valloc_t>;
 using btree_t   = GpuBTree::gpu_blink_tree<key_t, value_t, 16>;
-constexpr uint64_t kPoolNodes = 1ull << 28;
+constexpr uint64_t kPoolNodes = 1ull << 29;
+
+// Generous node estimate of a versioned workload: the initial tree at half-full leaves (two nodes
+// per 7 keys, interior levels included) plus 2 nodes per write (a version copy, a split now and
+// then; measured about 1).
+bool pool_estimate_ok(uint64_t initial, uint64_t writes) {
+  const uint64_t bound = 2 * (initial / 7 + 1) + 2 * writes + 4096;
+  if (bound <= kPoolNodes) return true;
+  std::fprintf(stderr, "ref_driver: workload could exceed the %llu-node pool (estimate %llu)\n",
+               (unsigned long long)kPoolNodes, (unsigned long long)bound);
+  return false;
+}
 
 void check(cudaError_t e, const char* what) {
   if (e != cudaSuccess) {
@@ -337,13 +351,8 @@ int run_c3(const args_t& a) {
   std::vector<uint32_t> keys(n), vals(n);
   mvbt_wl_distinct_keys(a.seed, 0, n, keys.data());
   mvbt_wl_values(keys.data(), n, (uint32_t)a.seed, vals.data());
-  for (const auto& c : combos) {
-    if (4 * (n / 6 + 1) + 4 * c.inserts + 1024 > kPoolNodes) {
-      std::fprintf(stderr, "ref_driver: workload could exceed the %llu-node pool\n",
-                   (unsigned long long)kPoolNodes);
-      return 2;
-    }
-  }
+  for (const auto& c : combos)
+    if (!pool_estimate_ok(n, c.inserts)) return 2;
   uint32_t *dk = dev_copy(keys), *dv = dev_copy(vals);
   cudaEvent_t e0, e1, e2, e3;
   check(cudaEventCreate(&e0), "event");
@@ -573,19 +582,16 @@ int run_c4(const args_t& a) {
   void* gen = mvbt_wl_mix_create(&p, a.seed, a.initial);
 
   // Generate every step first (untimed). Reads allocate nothing; a write adds about one node on
-  // average (a version copy per node and epoch, a split now and then). Refuse workloads whose
-  // generous estimate (4 nodes per write, 4x the initial tree) could reach the pool bound.
+  // average (a version copy per node and epoch, a split now and then).
   std::vector<step_t> steps;
-  uint64_t writes = 0;
+  uint64_t writes = 0, max_step_writes = 0;
   for (uint32_t k = 0; k < a.warmup + a.steps; ++k) {
     steps.push_back(split(gen, a.batches, stride));
-    writes += steps.back().ikeys.size() + steps.back().ekeys.size();
+    const uint64_t w = steps.back().ikeys.size() + steps.back().ekeys.size();
+    writes += w;
+    max_step_writes = std::max(max_step_writes, w);
   }
-  const uint64_t bound = 4 * (a.initial / 6 + 1) + 4 * writes + 1024;
-  if (bound > kPoolNodes) {
-    std::fprintf(stderr, "ref_driver: workload could exceed the %llu-node pool\n", (unsigned long long)kPoolNodes);
-    return 2;
-  }
+  if (!pool_estimate_ok(a.initial, writes)) return 2;
 
   uint32_t *dk = dev_copy(keys), *dv = dev_copy(vals);
   vtree_t tree;
@@ -612,6 +618,14 @@ int run_c4(const args_t& a) {
     if (k >= a.warmup) {
       timed_ms += elapsed_ms(e0, e1);
       timed_ops += steps[k].num_ops;
+    }
+    // the allocator's count (a blocking copy, outside the timed region): stop before the next
+    // step could pass the unchecked bound (4 nodes per write of the largest step as margin)
+    const uint64_t used = tree.get_num_tree_node();  // public (include/gpu_versioned_blink_tree.hpp:1096)
+    if (used + 4 * max_step_writes + 4096 > kPoolNodes) {
+      std::fprintf(stderr, "ref_driver: the pool holds %llu of %llu nodes after step %u\n",
+                   (unsigned long long)used, (unsigned long long)kPoolNodes, k);
+      return 2;
     }
     if (a.checksums) {
       uint64_t cs[3];

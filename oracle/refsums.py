@@ -1,6 +1,7 @@
 """Checksums of tree results, as oracle/ref_driver.cu computes them for the reference build, and a
-runner for that driver. Test infrastructure: the GPU tests compare this library's results with the
-reference implementation's on identical inputs through these sums.
+runner for that driver. Test infrastructure: the GPU tests and the benchmark's verification step
+compare this library's results with the reference implementation's on identical inputs through
+these sums.
 
 With mix(x) = the SplitMix64 finalizer of x + 0x9E3779B97F4A7C15 and i an op's index in its step:
   find  = sum over finds of mix(i << 32 | value)
@@ -17,8 +18,7 @@ from pathlib import Path
 
 import numpy as np
 
-ROOT = Path(__file__).resolve().parent.parent
-DRIVER = ROOT / "oracle" / "_ref" / "ref_driver"
+DRIVER = Path(__file__).resolve().parent / "_ref" / "ref_driver"
 
 _U = np.uint64
 

@@ -16,12 +16,14 @@ def pytest_configure(config):
 
 @pytest.fixture(scope="session", autouse=True)
 def _built_libraries():
-    """Builds libmvbt.so and the oracle if they are missing or stale (nvcc cross-compiles here)."""
+    """Builds libmvbt.so, the workload generator and the oracle if they are missing or stale (nvcc cross-compiles here)."""
     import importlib.util
     spec = importlib.util.spec_from_file_location("mvbt_build", ROOT / "mvgpubtree_b200" / "build.py")
     mod = importlib.util.module_from_spec(spec)
     spec.loader.exec_module(mod)
     mod.build()
+    from workload.build import build as build_workload
+    build_workload()
     from oracle.build import build as build_oracle
     build_oracle()
     yield

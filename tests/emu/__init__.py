@@ -122,7 +122,7 @@ class EmuTree:
         return pairs[: lo.size], counts[: lo.size]
 
     def run_batches(self, b, mode: int = 0):
-        """Runs mvgpubtree_b200.workload.Batches; returns (result, range_out words)."""
+        """Runs workload.Batches; returns (result, range_out words)."""
         result = np.zeros(b.num_ops, np.uint32)
         out = np.full(max(1, b.range_pairs) * 2, 0xFFFFFFFF, np.uint32)
         self.L.emu_batch_run(self.h, b.num_batches, b.batch_off, b.type, b.key, b.arg, b.out_off,

@@ -33,7 +33,7 @@ def test_emulated_tree_matches_reference_known_answers(name, kind, w):
 @pytest.mark.parametrize("w", [8, 16])
 def test_emulated_concurrent_insert_range_at_launch_snapshot(w):
     from emu import EmuTree
-    from mvgpubtree_b200 import workload as wl
+    import workload as wl
     import oracle
     seed, n0, L = 3, 3000, 8
     keys = wl.distinct_keys(seed, 0, n0)
@@ -67,7 +67,7 @@ def test_emulated_find_erase_newest_state(w):
     concurrent_find_erase): a find returns the key's value, or not-found only for an erased key
     (include/validation.hpp:106-149 of the reference accepts exactly these)."""
     from emu import EmuTree
-    from mvgpubtree_b200 import workload as wl
+    import workload as wl
     import oracle
     seed, n0 = 21, 6000
     keys = wl.distinct_keys(seed, 0, n0)
@@ -93,7 +93,7 @@ def test_emulated_reclaim_keeps_live_snapshots_and_reuses_nodes(w):
     at the newest state still match the oracle, freed copies are handed out again, and the
     allocation high-water mark stops growing."""
     from emu import EmuTree
-    from mvgpubtree_b200 import workload as wl
+    import workload as wl
     import oracle
     seed, n0 = 31, 3000
     keys = wl.distinct_keys(seed, 0, n0)
@@ -129,7 +129,7 @@ def test_emulated_reclaim_keeps_live_snapshots_and_reuses_nodes(w):
 
 def test_emulated_updates_erases_keep_old_snapshots():
     from emu import EmuTree
-    from mvgpubtree_b200 import workload as wl
+    import workload as wl
     import oracle
     seed, n0 = 9, 4000
     keys = wl.distinct_keys(seed, 0, n0)
@@ -158,7 +158,7 @@ def test_emulated_mixed_batches_match_oracle(mode, w):
     """Mixed erase/insert/find/range batches, one snapshot per batch (persistent worker loop
     with the writes-of-previous-batch dependency, and the per-batch mode)."""
     from emu import EmuTree
-    from mvgpubtree_b200 import workload as wl
+    import workload as wl
     import oracle
     seed, n0 = 12, 4000
     gen = wl.MixGenerator(seed, n0, stride=wl.stride_for(n0), batch_median=250, batch_min=1,

@@ -26,7 +26,7 @@ def host(t):
 def _setup(torch, seed, n0, W=8, pool=2 << 30):
     import mvgpubtree_b200 as mv
     import oracle
-    from mvgpubtree_b200 import workload as wl
+    import workload as wl
     init = wl.distinct_keys(seed, 0, n0)
     vals = wl.values_for(init, 0)
     t = mv.gpu_versioned_btree(pool_bytes=pool, tile_width=W)
@@ -49,7 +49,7 @@ def _run(torch, tree, plan, b, mode):
 @pytest.mark.parametrize("mode", [0, 1, 2])
 @pytest.mark.parametrize("w", [8, 16])
 def test_mixed_batches_match_oracle(torch, mode, w):
-    from mvgpubtree_b200 import workload as wl
+    import workload as wl
     seed, n0 = 31, 1 << 18
     t, m = _setup(torch, seed, n0, w)
     gen = wl.MixGenerator(seed, n0, stride=wl.stride_for(n0), batch_median=4096, batch_max=1 << 16)
@@ -67,7 +67,7 @@ def test_mixed_batches_match_oracle(torch, mode, w):
 def test_batches_see_every_earlier_batch_and_snapshots_advance(torch):
     """Tiny batches exercise the batch-to-batch dependency of the persistent launch."""
     import mvgpubtree_b200 as mv
-    from mvgpubtree_b200 import workload as wl
+    import workload as wl
     seed, n0 = 5, 1 << 14
     t, m = _setup(torch, seed, n0)
     e0 = t.take_snapshot(); m.take_snapshot()
@@ -84,7 +84,7 @@ def test_batches_see_every_earlier_batch_and_snapshots_advance(torch):
 def test_compact_range_output_packs_the_pairs_that_exist(torch, dest):
     """mvbt_batch_compact_ranges: every range query's first min(count, cap) pairs, in op order,
     packed contiguously (into device memory, or straight into pinned host memory)."""
-    from mvgpubtree_b200 import workload as wl
+    import workload as wl
     import mvgpubtree_b200 as mv
     initial, seed = 100_000, 29
     init = wl.distinct_keys(seed, 0, initial)
@@ -121,7 +121,7 @@ def test_compact_range_output_packs_the_pairs_that_exist(torch, dest):
 def test_compact_ranges_in_a_larger_plan_for_growing_op_counts(torch):
     """The packing scratch is sized for the plan's largest run on first use: packing a prefix of
     the ops and then all of them on a plan that holds more ops gives the right pairs both times."""
-    from mvgpubtree_b200 import workload as wl
+    import workload as wl
     import mvgpubtree_b200 as mv
     initial, seed = 100_000, 31
     init = wl.distinct_keys(seed, 0, initial)
@@ -151,3 +151,41 @@ def test_compact_ranges_in_a_larger_plan_for_growing_op_counts(torch):
         assert got_total == len(want), n
         assert np.array_equal(comp.cpu().numpy().view(np.uint32).reshape(-1, 2)[:got_total], want), n
     assert t.check_errors() == 0
+
+
+@pytest.mark.parametrize("w,bps", [(8, 0), (16, 6)])
+def test_full_c4_step_at_4M_keys_matches_oracle_and_plain(torch, w, bps):
+    """One step of the benchmark's batch law (256 batches, lognormal sizes median 16K ops, sigma
+    1.5, clipped [1K, 4M]; erase 10 % / insert 20 % / find 50 % / range 20 %, L geometric mean 32)
+    on a 4M-key tree: the persistent launch (at the benchmark's launch shapes) against the
+    partitioned oracle, and against the plain per-batch launch on an identical tree -- every find
+    value, range count and range-output word."""
+    import mvgpubtree_b200 as mv
+    import oracle
+    import os
+    import workload as wl
+    seed, n0 = 20240611, 4_000_000
+    init = wl.distinct_keys(seed, 0, n0)
+    vals = wl.values_for(init, 0)
+    gen = wl.MixGenerator(seed, n0, stride=wl.stride_for(40_000_000))
+    b = gen.generate(256)
+    assert b.num_ops > 5_000_000
+    outs = []
+    for mode in (mv.BATCH_PERSISTENT, mv.BATCH_PER_LAUNCH):
+        t = mv.gpu_versioned_btree(pool_bytes=4 << 30, tile_width=w,
+                                   blocks_per_sm=bps if mode == mv.BATCH_PERSISTENT else 0)
+        t.insert(dev(torch, init), dev(torch, vals))
+        plan = t.batch_plan(b.num_ops, 256)
+        outs.append(_run(torch, t, plan, b, mode))
+        rep = t.validate_tree_structure()
+        assert rep["violations"] == 0
+        plan.close()
+        t.close()
+    m = oracle.PartitionedMVMap(os.cpu_count() or 1, True)
+    m.insert(init, vals)
+    er, eo = m.run_batches(b)
+    m.close()
+    for name, (r, o) in zip(("persistent", "plain"), outs):
+        assert np.array_equal(r, er), f"{name}: {np.count_nonzero(r != er)} of {r.size} results differ"
+        assert np.array_equal(o, eo), f"{name}: {np.count_nonzero(o != eo)} range-output words differ"
+    assert rep["keys"] == n0 + 1 + int(np.count_nonzero(b.type == 1)) - int(np.count_nonzero(b.type == 2))

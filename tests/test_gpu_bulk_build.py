@@ -36,7 +36,7 @@ def find(torch, t, keys, ts=0xFFFFFFFF):
 @pytest.mark.parametrize("kind", ["blink", "versioned"])
 @pytest.mark.parametrize("w,fill", [(8, 8), (16, 13), (8, 2)])
 def test_bulk_built_tree_matches_oracle_and_keeps_working(torch, kind, w, fill):
-    from mvgpubtree_b200 import workload as wl
+    import workload as wl
     import mvgpubtree_b200 as mv
     import oracle
     seed, n = 5, 200_000 if fill > 2 else 20_000

@@ -44,7 +44,7 @@ def test_reference_known_answers(torch, name, kind, w):
 @pytest.mark.parametrize("n", [1 << 12, 1 << 20])
 def test_plain_tree_insert_find_matches_oracle(torch, w, n):
     """Plain B-link tree, n distinct uniform keys, n shuffled finds (half hits, half misses)."""
-    from mvgpubtree_b200 import workload as wl
+    import workload as wl
     import mvgpubtree_b200 as mv
     import oracle
     seed = 1234
@@ -68,7 +68,7 @@ def test_plain_tree_insert_find_matches_oracle(torch, w, n):
 @pytest.mark.parametrize("w", [8, 16])
 def test_versioned_updates_snapshots_match_oracle(torch, w):
     """Versioned tree: build, S0, update a subset, S1, finds at S0 and S1 (50 % hits)."""
-    from mvgpubtree_b200 import workload as wl
+    import workload as wl
     import mvgpubtree_b200 as mv
     import oracle
     seed, n, nu = 77, 1 << 18, 1 << 15
@@ -113,7 +113,7 @@ def _range_check(t, m, torch, lo, hi, cap, ts, concurrent=False):
 @pytest.mark.parametrize("w", [8, 16])
 @pytest.mark.parametrize("L", [8, 32, 128])
 def test_range_queries_at_snapshots_match_oracle(torch, w, L):
-    from mvgpubtree_b200 import workload as wl
+    import workload as wl
     import mvgpubtree_b200 as mv
     import oracle
     seed, n, nq = 99, 1 << 17, 1 << 14
@@ -140,7 +140,7 @@ def test_range_queries_at_snapshots_match_oracle(torch, w, L):
 @pytest.mark.parametrize("u", [0.05, 0.5, 0.9])
 def test_concurrent_insert_range_matches_oracle(torch, w, u):
     """One kernel of inserts + range queries; queries read the snapshot taken at launch."""
-    from mvgpubtree_b200 import workload as wl
+    import workload as wl
     import mvgpubtree_b200 as mv
     import oracle
     seed, n0, nops, L = 5, 1 << 18, 1 << 16, 32
@@ -179,7 +179,7 @@ def test_concurrent_insert_range_matches_oracle(torch, w, u):
 
 @pytest.mark.parametrize("kind", ["versioned", "blink"])
 def test_concurrent_find_erase(torch, kind):
-    from mvgpubtree_b200 import workload as wl
+    import workload as wl
     import mvgpubtree_b200 as mv
     import oracle
     seed, n0 = 8, 1 << 17
@@ -253,7 +253,7 @@ def test_edge_cases(torch, w):
 
 def test_pool_exhaustion_is_reported_not_hung(torch):
     """A tiny pool: inserts stop with MVBT_ERR_POOL_EXHAUSTED and the tree stays readable."""
-    from mvgpubtree_b200 import workload as wl
+    import workload as wl
     import mvgpubtree_b200 as mv
     t = mv.gpu_blink_tree(pool_bytes=1024 * 128, tile_width=8, chunk_nodes=8)
     keys = wl.distinct_keys(3, 0, 1 << 16)

@@ -43,7 +43,7 @@ def test_reclaim_needs_the_config_flag(torch):
 
 @pytest.mark.parametrize("w", [8, 16])
 def test_batches_with_reclaim_match_and_memory_stays_flat(torch, w):
-    from mvgpubtree_b200 import workload as wl
+    import workload as wl
     import mvgpubtree_b200 as mv
     initial, seed, nb, steps = 400_000, 9, 32, 8
     init = wl.distinct_keys(seed, 0, initial)
@@ -92,7 +92,7 @@ def test_batches_with_reclaim_match_and_memory_stays_flat(torch, w):
 
 @pytest.mark.parametrize("w", [8, 16])
 def test_reclaim_watermark_keeps_that_snapshot(torch, w):
-    from mvgpubtree_b200 import workload as wl
+    import workload as wl
     import mvgpubtree_b200 as mv
     import oracle
     seed, n0 = 13, 1 << 16

@@ -2,7 +2,7 @@
 
 oracle/_ref/ref_driver (built by oracle/ref_build.py from the reference's unmodified headers) runs
 the reference through its public host API; this library runs the same workload through its C ABI;
-checksums of every find result, range count and range pair are compared (tests/refbuild.py).
+checksums of every find result, range count and range pair are compared (oracle/refsums.py).
   * C1 shape: plain B-link tree, insert then finds (half present, half never inserted).
   * C2 shape: versioned tree, finds of the same queries at a snapshot before and after updates.
   * C3 shape: versioned tree, range queries at a snapshot before and after new inserts (a
@@ -14,7 +14,7 @@ checksums of every find result, range count and range pair are compared (tests/r
 import numpy as np
 import pytest
 
-from refbuild import DRIVER, find_sum, count_sum, pairs_sum, run_driver, step_sums
+from oracle.refsums import DRIVER, find_sum, count_sum, pairs_sum, run_driver, step_sums
 
 pytestmark = [pytest.mark.gpu,
               pytest.mark.skipif(not DRIVER.exists(), reason="reference build not present (oracle/ref_build.py)")]
@@ -40,7 +40,7 @@ def host(t):
 
 @pytest.mark.parametrize("w", [8, 16])
 def test_plain_tree_finds_match_reference_build(torch, w):
-    from mvgpubtree_b200 import workload as wl
+    import workload as wl
     import mvgpubtree_b200 as mv
     n, seed = 1 << 16, 7
     ref = run_driver("c1", "--n", str(n), "--seed", str(seed))
@@ -59,7 +59,7 @@ def test_plain_tree_finds_match_reference_build(torch, w):
 
 @pytest.mark.parametrize("w", [8, 16])
 def test_mixed_batches_match_reference_build(torch, w):
-    from mvgpubtree_b200 import workload as wl
+    import workload as wl
     import mvgpubtree_b200 as mv
     initial, seed, nb, warm, steps, chunks = 200_000, 5, 24, 1, 1, 64
     stride = wl.stride_for(initial)
@@ -109,7 +109,7 @@ def test_mixed_batches_match_reference_build(torch, w):
 def test_versioned_finds_at_two_snapshots_match_reference_build(torch, w):
     """C2 shape: insert, snapshot S0, in-place updates of an eighth of the keys, snapshot S1,
     the same hit/miss queries at S0 and at S1."""
-    from mvgpubtree_b200 import workload as wl
+    import workload as wl
     import mvgpubtree_b200 as mv
     n, seed = 1 << 17, 13
     u = n // 8
@@ -134,7 +134,7 @@ def test_versioned_finds_at_two_snapshots_match_reference_build(torch, w):
 
 
 def c3_case(seed, n, ops, u, L):
-    from mvgpubtree_b200 import workload as wl
+    import workload as wl
     stride = wl.stride_for(n)
     n_ins = int(ops * u)
     n_rq = ops - n_ins

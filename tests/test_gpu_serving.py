@@ -53,7 +53,7 @@ def make_tree(torch, mv, wl, initial, seed, w, reclaim):
 
 @pytest.mark.parametrize("w", [8, 16])
 def test_served_groups_match_oracle_and_alone_at_their_snapshot(torch, w):
-    from mvgpubtree_b200 import workload as wl
+    import workload as wl
     import mvgpubtree_b200 as mv
     import oracle
     initial, seed, R = 100_000, 91, 1500
@@ -107,7 +107,7 @@ def test_served_groups_match_oracle_and_alone_at_their_snapshot(torch, w):
 
 @pytest.mark.parametrize("w", [8, 16])
 def test_per_request_snapshots_match_oracle_and_alone(torch, w):
-    from mvgpubtree_b200 import workload as wl
+    import workload as wl
     import mvgpubtree_b200 as mv
     import oracle
     initial, seed, R = 100_000, 77, 1200
@@ -171,7 +171,7 @@ def test_per_request_snapshots_match_oracle_and_alone(torch, w):
 
 
 def test_serving_rejects_bad_traces(torch):
-    from mvgpubtree_b200 import workload as wl
+    import workload as wl
     import mvgpubtree_b200 as mv
     b, arrival = wl.serving_trace(5, 1000, 20, offered_mops=1.0, stride=wl.stride_for(1000))
     t = mv.gpu_versioned_btree(pool_bytes=1 << 26)

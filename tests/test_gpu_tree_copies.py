@@ -50,7 +50,7 @@ def build(torch, mv, wl, seed=41, n0=1 << 16, reclaim=True):
 
 
 def test_clone_reads_like_the_source_and_is_independent(torch):
-    from mvgpubtree_b200 import workload as wl
+    import workload as wl
     import mvgpubtree_b200 as mv
     t, keys, snaps = build(torch, mv, wl)
     c = t.clone()
@@ -66,7 +66,7 @@ def test_clone_reads_like_the_source_and_is_independent(torch):
 
 
 def test_saved_tree_loads_and_continues_identically(torch, tmp_path):
-    from mvgpubtree_b200 import workload as wl
+    import workload as wl
     import mvgpubtree_b200 as mv
     t, keys, snaps = build(torch, mv, wl, reclaim=True)
     path = tmp_path / "tree.mvbt"
@@ -88,7 +88,7 @@ def test_saved_tree_loads_and_continues_identically(torch, tmp_path):
 
 
 def test_launch_shapes_give_identical_batch_results(torch):
-    from mvgpubtree_b200 import workload as wl
+    import workload as wl
     import mvgpubtree_b200 as mv
     initial, seed = 200_000, 17
     init = wl.distinct_keys(seed, 0, initial)
@@ -121,7 +121,7 @@ def test_launch_shapes_give_identical_batch_results(torch):
 
 
 def test_autotune_leaves_the_tree_and_sets_the_plan(torch):
-    from mvgpubtree_b200 import workload as wl
+    import workload as wl
     from mvgpubtree_b200.autotune import autotune_batches, DEFAULT_CANDIDATES
     import mvgpubtree_b200 as mv
     initial, seed = 200_000, 23

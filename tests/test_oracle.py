@@ -67,7 +67,7 @@ def test_oracle_range_edges():
 def test_batch_runner_matches_step_by_step_replay():
     """orc_run_batches == snapshot / reads / writes issued one call at a time."""
     import oracle
-    from mvgpubtree_b200 import workload as wl
+    import workload as wl
     seed, n0 = 11, 20000
     gen = wl.MixGenerator(seed, n0, stride=wl.stride_for(n0), batch_median=512, batch_min=64,
                           batch_max=4096)
@@ -103,7 +103,7 @@ def test_batch_runner_matches_step_by_step_replay():
 @pytest.mark.parametrize("parts", [1, 3, 8])
 def test_partitioned_oracle_equals_sequential(parts):
     import oracle
-    from mvgpubtree_b200 import workload as wl
+    import workload as wl
     seed, n0 = 5, 50000
     gen = wl.MixGenerator(seed, n0, stride=wl.stride_for(n0) * 8, batch_median=2000)
     b = gen.generate(16)

@@ -2,7 +2,7 @@
 import numpy as np
 import pytest
 
-from mvgpubtree_b200 import workload as wl
+import workload as wl
 
 
 def test_distinct_keys_are_distinct_in_domain_and_deterministic():

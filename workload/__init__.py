@@ -1,4 +1,4 @@
-"""Deterministic synthetic workloads (numpy front-end of include/mvbt_workload.h).
+"""Deterministic synthetic workloads (numpy front-end of workload/mvbt_workload.h).
 
 The counterpart of the reference's key generator (include/rkg.hpp): distinct uniform keys in
 [1, 2^32 - 3], values fmix32(key ^ salt), range bounds [k, k + L * stride) saturated at
@@ -11,7 +11,11 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from . import lib
+from .build import LIB, build
+
+if not LIB.exists():
+    build()
+lib = ctypes.CDLL(str(LIB))
 
 _u32p = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
 _u64p = np.ctypeslib.ndpointer(dtype=np.uint64, flags="C_CONTIGUOUS")

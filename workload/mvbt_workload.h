@@ -1,5 +1,5 @@
 /*
- * mvbt_workload.h -- deterministic synthetic workloads for the tree (host functions of libmvbt.so).
+ * mvbt_workload.h -- deterministic synthetic workloads for the tree (host-only libworkload.so).
  *
  * The harness counterpart of the reference's include/rkg.hpp (generate_keys,
  * prep_experiment_find_with_exist_ratio, prep_experiment_range_query). All arrays here are HOST

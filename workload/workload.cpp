@@ -1,4 +1,4 @@
-// Deterministic synthetic workloads (host code of libmvbt.so).
+// Deterministic synthetic workloads (host-only library workload/libworkload.so).
 //
 // Counterpart of the reference's key generator include/rkg.hpp:77-97 (iota + std::shuffle with a
 // seeded mt19937) and its query preparation helpers (include/rkg.hpp:36-73). Keys here are
