@@ -79,8 +79,23 @@ typedef struct mvbt_config {
                            ring of 4 bytes per pool node each, rounded up to powers of two (8 to
                            16 bytes per node); 0 = keep every version, as the reference's bump
                            allocator does */
-  uint32_t reserved[3];
+  uint32_t frontend;    /* batch front-end of the bulk calls (MVBT_FRONTEND_*; 0 = AUTO) */
+  uint32_t reserved[2];
 } mvbt_config;
+
+/* Batch front-end of the bulk calls (insert, find, erase, range_query). SORTED first sorts the
+ * call's keys (a stable radix sort on the device: all 32 bits for writes, so a repeated key's last
+ * occurrence in the array wins; the top 24 bits for reads, which only need locality) and gives
+ * each tile a contiguous run of them; each op then starts its descent at the deepest node of the
+ * previous op's path that covers its key, and results go back to the caller's positions. UNSORTED
+ * runs the ops in the caller's order, each from the root. AUTO takes SORTED when the call is large
+ * and dense against the tree (at least 2^16 ops and one op per 128 keys), where neighbouring ops
+ * share nodes. Results are the same either way (for a repeated key in one insert call, UNSORTED
+ * leaves which value wins unspecified, as the reference does). The sort's scratch (16 bytes per op)
+ * comes from a stream-ordered memory pool of the library. No counterpart in the reference. */
+#define MVBT_FRONTEND_AUTO 0u
+#define MVBT_FRONTEND_UNSORTED 1u
+#define MVBT_FRONTEND_SORTED 2u
 
 /* Structural report of a host walk over a copy of the node pool (mvbt_validate). */
 typedef struct mvbt_report {
@@ -114,6 +129,10 @@ int mvbt_create(int kind, const mvbt_config* cfg, mvbt_tree** out);
 
 /* Frees the pool and all buffers. Replaces the shared_ptr teardown of the reference handles. */
 int mvbt_destroy(mvbt_tree* tree);
+
+/* Sets the batch front-end of the bulk calls (MVBT_FRONTEND_*), as config.frontend does at
+ * creation. Host-side only; affects calls issued afterwards. No counterpart in the reference. */
+int mvbt_set_frontend(mvbt_tree* tree, uint32_t frontend);
 
 /* Upserts n pairs. in_place selects the reference's ViB (1) or VoB (0) insert; both keep every
  * version an older snapshot can read, so results are identical; blink trees ignore it.

@@ -647,6 +647,39 @@ MVBT_COLD void retire_logged(control_block* c, uint32_t copy) {
     atomicAdd(&c->stat_log_dropped, 1ull);
 }
 
+// Path memory of a tile that runs ops in ascending key order (the sorted batch front-end): lane l
+// remembers the node it last passed at level l and that node's fences [low, high). The next op
+// starts at the lowest remembered node whose fences cover its key instead of at the anchor, so a
+// run of nearby keys shares the upper levels and often the leaf. Any node whose low fence is <= the
+// key is a valid start (low fences never change; a split that lowered the high fence since the
+// node was read is repaired by the right-link chase), and a remembered version is the one a
+// snapshot read resolved to, so its children route that snapshot. Levels >= W are not kept.
+template <int W>
+struct finger {
+  uint32_t idx  = kNone;
+  uint32_t low  = 0;
+  uint32_t high = 0;
+  // Lowest remembered node covering key, or the anchor.
+  template <class Tile>
+  MVBT_DEV uint32_t start_for(uint32_t key, const Tile& t) const {
+    const uint32_t m = t.ballot(idx != kNone && low <= key && key < high);
+    return m ? t.shfl(idx, __ffs(m) - 1) : kAnchor;
+  }
+  template <class Tile>
+  MVBT_DEV void record(uint32_t level, uint32_t node, uint32_t lo, uint32_t hi, const Tile& t) {
+    if (t.thread_rank() == (int)level) {
+      idx  = node;
+      low  = lo;
+      high = hi;
+    }
+  }
+  // The interior node remembered at `level` (kNone if none): the parent hint of insert_at.
+  template <class Tile>
+  MVBT_DEV uint32_t at(uint32_t level, const Tile& t) const {
+    return level < (uint32_t)W ? t.shfl(idx, (int)level) : kNone;
+  }
+};
+
 struct device_tree {
   uint32_t* pool;       // node words; node i starts at pool + 32 * i
   control_block* ctl;   // device control block
@@ -970,9 +1003,12 @@ struct device_tree {
   // ------------------------------------------------------------------------------------------
   // Point lookup at snapshot ts (kLatest = newest). concurrent = writers may run meanwhile.
   // ------------------------------------------------------------------------------------------
+  // f (nullable): path memory of a sorted run; every node the lookup passes on key's route is
+  // recorded in it (the version a snapshot read resolved to).
   template <int W, class Tile>
   MVBT_DEV uint32_t cooperative_find(uint32_t key, const Tile& t, uint32_t ts = kLatest,
-                                     bool concurrent = false, uint32_t start = kAnchor) const {
+                                     bool concurrent = false, uint32_t start = kAnchor,
+                                     finger<W>* f = nullptr) const {
     const bool snap   = versioned && ts != kLatest;
     const bool seqlk  = !snap && concurrent;  // newest state under writers: read leaves locked-free
     uint32_t idx      = start;  // the anchor, or a node on key's route found earlier
@@ -1013,8 +1049,10 @@ struct device_tree {
           leaf_next = true;  // reached without knowing it was a leaf: read it again, consistently
           continue;
         }
+        if (f) f->record(0, idx, h.low, h.high, t);
         return leaf_value<W>(n, key, t);
       }
+      if (f) f->record(h.level(), idx, h.low, h.high, t);
       leaf_next = h.level() == 1;
       idx       = child_for<W>(n, key, t);
       if (idx == kNone) {
@@ -1030,10 +1068,11 @@ struct device_tree {
   // Range query [lo, hi) at snapshot ts. Writes at most cap pairs {key, value} ascending at out
   // (nullable) and returns the full count.
   // ------------------------------------------------------------------------------------------
+  // f (nullable): path memory of a sorted run (as in cooperative_find), recorded along lo's route.
   template <int W, class Tile>
   MVBT_DEV uint32_t cooperative_range_query(uint32_t lo, uint32_t hi, const Tile& t, uint32_t ts,
                                             uint2* out, uint32_t cap, bool concurrent = false,
-                                            uint32_t start = kAnchor) const {
+                                            uint32_t start = kAnchor, finger<W>* f = nullptr) const {
     constexpr int P = 16 / W;
     if (hi <= lo) return 0;
     const bool snap  = versioned && ts != kLatest;
@@ -1082,8 +1121,10 @@ struct device_tree {
           leaf_next = true;
           continue;
         }
+        if (f) f->record(0, idx, h.low, h.high, t);
         break;
       }
+      if (f) f->record(h.level(), idx, h.low, h.high, t);
       leaf_next = h.level() == 1;
       idx       = child_for<W>(n, lo, t);
       if (idx == kNone) {
@@ -1157,6 +1198,51 @@ struct device_tree {
   // ------------------------------------------------------------------------------------------
   // Writers
   // ------------------------------------------------------------------------------------------
+  // Descent of a writer in a sorted run: like descend_for_write, but it starts at the lowest node
+  // of f covering key and records every node it passes (the leaf at level 0) in f, which then
+  // serves as the path of parent hints (insert_at with path0 = f's per-lane nodes).
+  template <int W, class Tile>
+  MVBT_DEV uint32_t descend_with_finger(uint32_t key, finger<W>& f, const Tile& t) const {
+    uint32_t idx = f.start_for(key, t);
+    node_regs<W> n;
+    for (uint32_t step = 0; step < kMaxSteps; ++step) {
+      if (!valid(idx, t)) return kNone;
+      load<W>(idx, n, true, t);
+      header h = get_header<W>(n, t);
+      if (key < h.low) {  // a torn read upstream routed too far right: start over from the anchor
+        idx = kAnchor;
+        continue;
+      }
+      if (key >= h.high && h.sibling() != kNone) {
+        idx = h.sibling();
+        continue;
+      }
+      f.record(h.level(), idx, h.low, h.high, t);
+      if (h.is_leaf()) return idx;
+      idx = child_for<W>(n, key, t);
+      if (idx == kNone) idx = kAnchor;
+    }
+    if (t.thread_rank() == 0) set_error(kErrStepLimit, 8);
+    return kNone;
+  }
+
+  // Insert / erase of one key of a sorted run (the sorted batch front-end): the descent starts
+  // from the run's path memory f instead of the anchor.
+  template <int W, class Tile>
+  MVBT_DEV bool insert_in_run(uint32_t key, uint32_t value, const Tile& t, uint32_t E, finger<W>& f) const {
+    if (key == kEmptyKey) return false;
+    const uint32_t leaf = descend_with_finger<W>(key, f, t);
+    if (leaf == kNone) return false;
+    return insert_at<W>(key, value, t, E, leaf, f.idx, kNone, (uint32_t)W - 1);
+  }
+  template <int W, class Tile>
+  MVBT_DEV bool erase_in_run(uint32_t key, const Tile& t, uint32_t E, finger<W>& f) const {
+    if (key == kEmptyKey) return false;
+    const uint32_t leaf = descend_with_finger<W>(key, f, t);
+    if (leaf == kNone) return false;
+    return erase_at<W>(key, t, E, leaf);
+  }
+
   // Descends to the leaf for key (newest versions, strong loads), recording in `path` the
   // interior node visited at each level: lane l holds level l in path0 and level l + W in path1.
   template <int W, class Tile>

@@ -17,10 +17,12 @@ __all__ = [
     "LATEST", "NOT_FOUND", "MVBTError", "lib", "library_path", "gpu_blink_tree",
     "gpu_versioned_btree", "gpu_versioned_blink_tree", "pair_dtype_words", "BatchPlan",
     "BATCH_PERSISTENT", "BATCH_PER_LAUNCH", "BATCH_GRAPH", "NOALLOC_MAX_OPS", "NOALLOC_MAX_BATCHES",
+    "FRONTEND_AUTO", "FRONTEND_UNSORTED", "FRONTEND_SORTED",
     "RECLAIM_ALL", "SERVE_SNAPSHOT_PER_BATCH", "SERVE_SNAPSHOT_PER_REQUEST", "load",
 ]
 
 LATEST = 0xFFFFFFFF
+FRONTEND_AUTO, FRONTEND_UNSORTED, FRONTEND_SORTED = 0, 1, 2  # MVBT_FRONTEND_*
 NOT_FOUND = 0xFFFFFFFF
 pair_dtype_words = 2  # a result pair is two uint32 words {key, value}
 
@@ -41,7 +43,7 @@ class mvbt_config(ctypes.Structure):
     _fields_ = [("pool_bytes", _u64), ("device", _i32), ("tile_width", _i32),
                 ("block_size", _i32), ("spin_limit", _u32), ("chunk_nodes", _u32),
                 ("blocks_per_sm", _u32), ("max_blocks", _u32), ("wait_ms", _u32),
-                ("reclaim", _u32), ("reserved", _u32 * 3)]
+                ("reclaim", _u32), ("frontend", _u32), ("reserved", _u32 * 2)]
 
 
 class mvbt_report(ctypes.Structure):
@@ -78,6 +80,7 @@ _P = _vp
 _sig("mvbt_config_init", None, ctypes.POINTER(mvbt_config))
 _sig("mvbt_create", ctypes.c_int, ctypes.c_int, ctypes.POINTER(mvbt_config), ctypes.POINTER(_vp))
 _sig("mvbt_destroy", ctypes.c_int, _vp)
+_sig("mvbt_set_frontend", ctypes.c_int, _vp, _u32)
 _sig("mvbt_insert", ctypes.c_int, _vp, _P, _P, _u32, _vp, ctypes.c_int)
 _sig("mvbt_find", ctypes.c_int, _vp, _P, _P, _u32, _u32, _vp, ctypes.c_int)
 _sig("mvbt_erase", ctypes.c_int, _vp, _P, _u32, _vp, ctypes.c_int)
@@ -195,7 +198,7 @@ class _TreeBase:
     def __init__(self, pool_bytes: int = 4 << 30, tile_width: int = 8, device: int | None = None,
                  block_size: int = 256, spin_limit: int = 0, chunk_nodes: int = 0,
                  blocks_per_sm: int = 0, max_blocks: int = 0, wait_ms: int = 0,
-                 reclaim: bool = False):
+                 reclaim: bool = False, frontend: int = 0):
         cfg = mvbt_config()
         lib.mvbt_config_init(ctypes.byref(cfg))
         cfg.pool_bytes = int(pool_bytes)
@@ -209,6 +212,7 @@ class _TreeBase:
         if wait_ms:
             cfg.wait_ms = int(wait_ms)
         cfg.reclaim = 1 if reclaim else 0
+        cfg.frontend = int(frontend)
         h = _vp()
         _check(lib.mvbt_create(self._kind, ctypes.byref(cfg), ctypes.byref(h)), "mvbt_create")
         self._h = h
@@ -231,6 +235,11 @@ class _TreeBase:
         n = _numel(keys) if num_keys is None else int(num_keys)
         _check(lib.mvbt_bulk_build(self._h, _ptr(keys, name="keys"), _ptr(values, name="values"), n,
                                    int(fill), _stream(stream)), "bulk_build")
+
+    def set_frontend(self, frontend: int) -> None:
+        """Batch front-end of the bulk calls: FRONTEND_AUTO, FRONTEND_UNSORTED or FRONTEND_SORTED
+        (sort the call's keys on the device and run each tile over a contiguous run of them)."""
+        _check(lib.mvbt_set_frontend(self._h, int(frontend)), "set_frontend")
 
     def clone(self) -> "_TreeBase":
         """A copy of the tree (every version, allocator and reclamation state) with the same

@@ -10,11 +10,13 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
 #include "mvbt.h"
 #include "mvbt_device.cuh"
+#include "mvbt_sort.h"
 
 namespace cg = cooperative_groups;
 using mvbt::control_block;
@@ -38,6 +40,7 @@ struct mvbt_tree {
   uint32_t blocks_per_sm;
   uint32_t max_blocks;
   uint32_t wait_ms;
+  uint32_t frontend = MVBT_FRONTEND_AUTO;  // batch front-end of the bulk calls (MVBT_FRONTEND_*)
   // Upper bound on the keys ever written into the tree (host-side, by the calls that write):
   // leaves are never merged, so it bounds the leaf count from above too. Bulk inserts into a tree
   // that is small against the batch are split by it (insert_launches).
@@ -239,6 +242,103 @@ __global__ void __launch_bounds__(256)
 }
 
 // ----------------------------------------------------------------------------------------------
+// Sorted batch front-end: the ops of a call sorted by key (mvbt_sort.cu), each tile running one
+// contiguous run of them with its path memory (mvbt::finger), results scattered back to the
+// caller's positions (spos = sorted position -> input position).
+// ----------------------------------------------------------------------------------------------
+// The calling tile's run of sorted positions [begin, end): equal shares of n over the grid.
+template <int W>
+__device__ __forceinline__ void tile_run(uint64_t n, uint64_t& begin, uint64_t& end) {
+  const uint64_t per = (n + num_tiles<W>() - 1) / num_tiles<W>();
+  begin              = first_tile<W>() * per;
+  end                = begin + per < n ? begin + per : n;
+}
+
+template <int W, bool kStrong>
+__global__ void __launch_bounds__(256) k_find_sorted(device_tree T, const uint32_t* __restrict__ skeys,
+                                                     const uint32_t* __restrict__ spos,
+                                                     uint32_t* __restrict__ out, uint32_t n, uint32_t ts) {
+  auto tile = cg::tiled_partition<W>(cg::this_thread_block());
+  uint64_t i, end;
+  tile_run<W>(n, i, end);
+  mvbt::finger<W> f;
+  for (; i < end; ++i) {
+    const uint32_t key = skeys[i];
+    const uint32_t v   = T.cooperative_find<W>(key, tile, ts, kStrong, f.start_for(key, tile), &f);
+    if (tile.thread_rank() == 0) out[spos[i]] = v;
+  }
+}
+
+template <int W, bool kStrong>
+__global__ void __launch_bounds__(256) k_range_sorted(device_tree T, const uint32_t* __restrict__ slower,
+                                                      const uint32_t* __restrict__ spos,
+                                                      const uint32_t* __restrict__ upper, uint2* result,
+                                                      uint32_t* counts, uint32_t avg_len, uint32_t n,
+                                                      uint32_t ts) {
+  auto tile = cg::tiled_partition<W>(cg::this_thread_block());
+  uint64_t i, end;
+  tile_run<W>(n, i, end);
+  mvbt::finger<W> f;
+  for (; i < end; ++i) {
+    const uint32_t lo = slower[i], p = spos[i];
+    uint2* out        = result ? result + p * (uint64_t)avg_len : nullptr;
+    const uint32_t c  = T.cooperative_range_query<W>(lo, upper[p], tile, ts, out, avg_len, kStrong,
+                                                     f.start_for(lo, tile), &f);
+    if (counts && tile.thread_rank() == 0) counts[p] = c;
+  }
+}
+
+// A key repeated in one insert call: only its last occurrence in the caller's array is applied
+// (the stable sort keeps equal keys in input order), as applying them in order would leave it.
+__device__ __forceinline__ bool superseded(const uint32_t* skeys, uint64_t i, uint64_t n) {
+  return i + 1 < n && skeys[i + 1] == skeys[i];
+}
+
+template <int W>
+__global__ void __launch_bounds__(256) k_insert_sorted(device_tree T, const uint32_t* __restrict__ skeys,
+                                                       const uint32_t* __restrict__ spos,
+                                                       const uint32_t* __restrict__ values, uint32_t n) {
+  auto tile        = cg::tiled_partition<W>(cg::this_thread_block());
+  const uint32_t E = T.versioned ? T.current_epoch() : 0u;
+  uint64_t i, end;
+  tile_run<W>(n, i, end);
+  mvbt::finger<W> f;
+  for (; i < end; ++i) {
+    if (superseded(skeys, i, n)) continue;
+    T.insert_in_run<W>(skeys[i], values[spos[i]], tile, E, f);
+  }
+}
+
+// Growth phase of a sorted insert into a tree that has fewer leaves than the grid has tiles: m
+// evenly spaced keys of the sorted array, one per tile, so that no two tiles queue on one leaf.
+// The final contiguous-run launch applies them again (an upsert of the same value changes
+// nothing visible).
+template <int W>
+__global__ void __launch_bounds__(256) k_insert_spread(device_tree T, const uint32_t* __restrict__ skeys,
+                                                       const uint32_t* __restrict__ spos,
+                                                       const uint32_t* __restrict__ values, uint32_t n,
+                                                       uint32_t m) {
+  auto tile        = cg::tiled_partition<W>(cg::this_thread_block());
+  const uint32_t E = T.versioned ? T.current_epoch() : 0u;
+  for (uint64_t j = first_tile<W>(); j < m; j += num_tiles<W>()) {
+    const uint64_t i = j * n / m;
+    if (superseded(skeys, i, n)) continue;
+    T.cooperative_insert<W>(skeys[i], values[spos[i]], tile, E);
+  }
+}
+
+template <int W>
+__global__ void __launch_bounds__(256) k_erase_sorted(device_tree T, const uint32_t* __restrict__ skeys,
+                                                      uint32_t n) {
+  auto tile        = cg::tiled_partition<W>(cg::this_thread_block());
+  const uint32_t E = T.versioned ? T.current_epoch() : 0u;
+  uint64_t i, end;
+  tile_run<W>(n, i, end);
+  mvbt::finger<W> f;
+  for (; i < end; ++i) T.erase_in_run<W>(skeys[i], tile, E, f);
+}
+
+// ----------------------------------------------------------------------------------------------
 // Launch helpers
 // ----------------------------------------------------------------------------------------------
 template <class K>
@@ -289,6 +389,98 @@ int insert_launches(mvbt_tree* t, const uint32_t* keys, const uint32_t* values, 
     if (st) return st;
     done += chunk;
     t->grown += chunk;
+  }
+  return MVBT_OK;
+}
+
+// ---- sorted batch front-end: host side ----
+// Whether a bulk call of n ops takes the sorted front-end (MVBT_FRONTEND_AUTO: a large call that
+// is dense against the tree, so that neighbouring sorted ops share nodes).
+bool use_sorted(const mvbt_tree* t, uint32_t n) {
+  if (t->frontend == MVBT_FRONTEND_SORTED) return n > 1;
+  if (t->frontend == MVBT_FRONTEND_UNSORTED) return false;
+  return n >= (1u << 16) && (uint64_t)n * 128 >= t->grown;
+}
+
+// A stream-ordered memory pool per device for the sort's scratch: no device-wide synchronisation,
+// and freed blocks stay cached in the pool for the next call (up to kPoolKeepBytes).
+constexpr int kMaxDevices           = 64;
+constexpr uint64_t kPoolKeepBytes   = 4ull << 30;
+cudaMemPool_t g_sort_pool[kMaxDevices] = {};
+std::mutex g_sort_pool_mu;
+
+int sort_pool(int dev, cudaMemPool_t* out) {
+  if (dev < 0 || dev >= kMaxDevices) return fail(MVBT_ERR_BAD_ARG, "device ordinal out of range");
+  std::lock_guard<std::mutex> lk(g_sort_pool_mu);
+  if (!g_sort_pool[dev]) {
+    cudaMemPoolProps props = {};
+    props.allocType        = cudaMemAllocationTypePinned;
+    props.location.type    = cudaMemLocationTypeDevice;
+    props.location.id      = dev;
+    MVBT_CUDA_TRY(cudaMemPoolCreate(&g_sort_pool[dev], &props));
+    uint64_t keep = kPoolKeepBytes;
+    MVBT_CUDA_TRY(cudaMemPoolSetAttribute(g_sort_pool[dev], cudaMemPoolAttrReleaseThreshold, &keep));
+  }
+  *out = g_sort_pool[dev];
+  return MVBT_OK;
+}
+
+// The keys of a call in ascending order with their input positions, in pool memory released by
+// release() (stream-ordered, after the kernels that read it).
+struct sorted_ops {
+  uint32_t* keys = nullptr;
+  uint32_t* pos  = nullptr;
+  void* mem      = nullptr;
+  int release(cudaStream_t s) {
+    if (mem && cudaFreeAsync(mem, s) != cudaSuccess) return fail(MVBT_ERR_CUDA, "cudaFreeAsync of sort scratch");
+    mem = nullptr;
+    return MVBT_OK;
+  }
+};
+
+int sort_ops(mvbt_tree* t, const uint32_t* keys, uint32_t n, int low_bit, cudaStream_t s, sorted_ops* out) {
+  cudaMemPool_t pool;
+  int st = sort_pool(t->device, &pool);
+  if (st) return st;
+  const uint64_t words = 4ull * n + mvbt_sort::scratch_words(n);
+  void* mem            = nullptr;
+  if (cudaMallocFromPoolAsync(&mem, words * 4, pool, s) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(MVBT_ERR_OUT_OF_MEMORY, "sort scratch: cudaMallocFromPoolAsync failed");
+  }
+  uint32_t* w = static_cast<uint32_t*>(mem);
+  out->mem    = mem;
+  out->keys   = w;
+  out->pos    = w + n;
+  if (mvbt_sort::sort_pairs(keys, n, low_bit, w, w + n, w + 2ull * n, w + 3ull * n, w + 4ull * n, s)) {
+    out->release(s);
+    return fail(MVBT_ERR_CUDA, std::string("sort launch: ") + cudaGetErrorString(cudaGetLastError()));
+  }
+  return MVBT_OK;
+}
+
+constexpr int kReadSortLowBit = 8;  // reads: order by the top 24 bits (locality is all they need)
+
+template <int W>
+int insert_sorted_launches(mvbt_tree* t, const sorted_ops& so, const uint32_t* values, uint32_t n, cudaStream_t s) {
+  const uint64_t full  = grid_for(t, k_insert_sorted<W>, n);
+  const uint64_t tiles = (uint64_t)t->block_size / W;
+  uint64_t spread      = 0;
+  while (t->grown / 10 < full * tiles && spread < n) {  // fewer leaves than tiles: spread first
+    uint64_t blocks = std::max<uint64_t>(1, (t->grown / 10) / tiles);
+    blocks          = std::min(blocks, full);
+    uint64_t m      = std::min<uint64_t>(n, std::max<uint64_t>(t->grown, blocks * tiles * 16));
+    k_insert_spread<W><<<(unsigned)blocks, t->block_size, 0, s>>>(t->view(), so.keys, so.pos, values, n, (uint32_t)m);
+    int st = check_launch();
+    if (st) return st;
+    t->grown += m;
+    spread = m;
+  }
+  if (spread < n) {
+    k_insert_sorted<W><<<(unsigned)full, t->block_size, 0, s>>>(t->view(), so.keys, so.pos, values, n);
+    int st = check_launch();
+    if (st) return st;
+    t->grown += n - spread;
   }
   return MVBT_OK;
 }
@@ -365,6 +557,7 @@ int mvbt_create(int kind, const mvbt_config* cfg_in, mvbt_tree** out) {
   t->max_blocks    = cfg.max_blocks;
   t->wait_ms       = cfg.wait_ms ? cfg.wait_ms : 2000u;
   if (t->wait_ms > 4000u) t->wait_ms = 4000u;  // wait_ns is a 32-bit ns count
+  t->frontend      = cfg.frontend <= MVBT_FRONTEND_SORTED ? cfg.frontend : MVBT_FRONTEND_AUTO;
   cudaDeviceProp prop;
   cudaError_t e = cudaGetDeviceProperties(&prop, dev);
   if (e != cudaSuccess) {
@@ -569,6 +762,7 @@ static mvbt_config config_of(const mvbt_tree* t) {
   c.max_blocks    = t->max_blocks;
   c.wait_ms       = t->wait_ms;
   c.reclaim       = t->retire_log ? 1u : 0u;
+  c.frontend      = t->frontend;
   return c;
 }
 
@@ -748,6 +942,15 @@ int mvbt_insert(mvbt_tree* t, const uint32_t* keys, const uint32_t* values, uint
   if (!t || (n && (!keys || !values))) return fail(MVBT_ERR_BAD_ARG, "null argument");
   if (n == 0) return MVBT_OK;
   cudaStream_t s = as_stream(stream);
+  if (use_sorted(t, n)) {
+    sorted_ops so;
+    int st = sort_ops(t, keys, n, 0, s, &so);
+    if (st) return st;
+    st = t->tile_width == 8 ? insert_sorted_launches<8>(t, so, values, n, s)
+                            : insert_sorted_launches<16>(t, so, values, n, s);
+    const int rs = so.release(s);
+    return st ? st : rs;
+  }
   return t->tile_width == 8 ? insert_launches<8>(t, keys, values, n, s) : insert_launches<16>(t, keys, values, n, s);
 }
 
@@ -758,6 +961,22 @@ int mvbt_find(mvbt_tree* t, const uint32_t* keys, uint32_t* values, uint32_t n, 
   if (t->kind == MVBT_KIND_BLINK) ts = mvbt::kLatest;
   cudaStream_t s = as_stream(stream);
   const int bs   = t->block_size;
+  if (use_sorted(t, n)) {
+    sorted_ops so;
+    int st = sort_ops(t, keys, n, kReadSortLowBit, s, &so);
+    if (st) return st;
+    const device_tree v = t->view();
+    if (t->tile_width == 8) {
+      if (concurrent) k_find_sorted<8, true><<<grid_for(t, k_find_sorted<8, true>, n), bs, 0, s>>>(v, so.keys, so.pos, values, n, ts);
+      else k_find_sorted<8, false><<<grid_for(t, k_find_sorted<8, false>, n), bs, 0, s>>>(v, so.keys, so.pos, values, n, ts);
+    } else {
+      if (concurrent) k_find_sorted<16, true><<<grid_for(t, k_find_sorted<16, true>, n), bs, 0, s>>>(v, so.keys, so.pos, values, n, ts);
+      else k_find_sorted<16, false><<<grid_for(t, k_find_sorted<16, false>, n), bs, 0, s>>>(v, so.keys, so.pos, values, n, ts);
+    }
+    st = check_launch();
+    const int rs = so.release(s);
+    return st ? st : rs;
+  }
   if (t->tile_width == 8) {
     if (concurrent) k_find<8, true><<<grid_for(t, k_find<8, true>, n), bs, 0, s>>>(t->view(), keys, values, n, ts);
     else k_find<8, false><<<grid_for(t, k_find<8, false>, n), bs, 0, s>>>(t->view(), keys, values, n, ts);
@@ -773,6 +992,18 @@ int mvbt_erase(mvbt_tree* t, const uint32_t* keys, uint32_t n, void* stream, int
   if (!t || (n && !keys)) return fail(MVBT_ERR_BAD_ARG, "null argument");
   if (n == 0) return MVBT_OK;
   cudaStream_t s = as_stream(stream);
+  if (use_sorted(t, n)) {
+    sorted_ops so;
+    int st = sort_ops(t, keys, n, 0, s, &so);
+    if (st) return st;
+    if (t->tile_width == 8)
+      k_erase_sorted<8><<<grid_for(t, k_erase_sorted<8>, n), t->block_size, 0, s>>>(t->view(), so.keys, n);
+    else
+      k_erase_sorted<16><<<grid_for(t, k_erase_sorted<16>, n), t->block_size, 0, s>>>(t->view(), so.keys, n);
+    st = check_launch();
+    const int rs = so.release(s);
+    return st ? st : rs;
+  }
   if (t->tile_width == 8) {
     k_erase<8><<<grid_for(t, k_erase<8>, n), t->block_size, 0, s>>>(t->view(), keys, n);
   } else {
@@ -790,6 +1021,22 @@ int mvbt_range_query(mvbt_tree* t, const uint32_t* lower, const uint32_t* upper,
   cudaStream_t s = as_stream(stream);
   uint2* out     = reinterpret_cast<uint2*>(result);
   const int bs   = t->block_size;
+  if (use_sorted(t, n)) {
+    sorted_ops so;
+    int st = sort_ops(t, lower, n, kReadSortLowBit, s, &so);
+    if (st) return st;
+    const device_tree v = t->view();
+    if (t->tile_width == 8) {
+      if (concurrent) k_range_sorted<8, true><<<grid_for(t, k_range_sorted<8, true>, n), bs, 0, s>>>(v, so.keys, so.pos, upper, out, counts, avg_len, n, ts);
+      else k_range_sorted<8, false><<<grid_for(t, k_range_sorted<8, false>, n), bs, 0, s>>>(v, so.keys, so.pos, upper, out, counts, avg_len, n, ts);
+    } else {
+      if (concurrent) k_range_sorted<16, true><<<grid_for(t, k_range_sorted<16, true>, n), bs, 0, s>>>(v, so.keys, so.pos, upper, out, counts, avg_len, n, ts);
+      else k_range_sorted<16, false><<<grid_for(t, k_range_sorted<16, false>, n), bs, 0, s>>>(v, so.keys, so.pos, upper, out, counts, avg_len, n, ts);
+    }
+    st = check_launch();
+    const int rs = so.release(s);
+    return st ? st : rs;
+  }
   if (t->tile_width == 8) {
     if (concurrent) k_range<8, true><<<grid_for(t, k_range<8, true>, n), bs, 0, s>>>(t->view(), lower, upper, out, counts, avg_len, n, ts);
     else k_range<8, false><<<grid_for(t, k_range<8, false>, n), bs, 0, s>>>(t->view(), lower, upper, out, counts, avg_len, n, ts);
@@ -798,6 +1045,13 @@ int mvbt_range_query(mvbt_tree* t, const uint32_t* lower, const uint32_t* upper,
     else k_range<16, false><<<grid_for(t, k_range<16, false>, n), bs, 0, s>>>(t->view(), lower, upper, out, counts, avg_len, n, ts);
   }
   return check_launch();
+}
+
+int mvbt_set_frontend(mvbt_tree* t, uint32_t frontend) {
+  if (!t) return fail(MVBT_ERR_BAD_ARG, "null tree");
+  if (frontend > MVBT_FRONTEND_SORTED) return fail(MVBT_ERR_BAD_ARG, "unknown front-end");
+  t->frontend = frontend;
+  return MVBT_OK;
 }
 
 int mvbt_take_snapshot_async(mvbt_tree* t, void* stream, uint32_t* d_out) {

@@ -259,6 +259,54 @@ void emu_insert_range(void* h, const uint32_t* keys, const uint32_t* vals, uint6
   }));
 }
 
+// Sorted runs (the sorted batch front-end): keys[0, n) ascending, pos[i] = the input position of
+// keys[i]; each of `tiles` tiles takes one contiguous share of the run and keeps its path memory
+// (mvbt::finger, one per lane, as registers are on the GPU). kind: 0 find, 1 range, 2 insert (a
+// repeated key: its last occurrence wins), 3 erase.
+void emu_sorted_run(void* h, int kind, const uint32_t* keys, const uint32_t* pos, const uint32_t* arg,
+                    uint32_t* out, uint32_t* pairs, uint32_t avg_len, uint64_t n, uint32_t ts, int tiles, int W) {
+  auto* t = static_cast<emu_tree*>(h);
+  auto v  = t->view();
+  if (!v.versioned) ts = mvbt::kLatest;
+  if (n == 0) return;
+  if (tiles < 1) tiles = 1;
+  const uint64_t per = (n + tiles - 1) / tiles;
+  EMU_DISPATCH(W, {
+    std::vector<std::unique_ptr<tile_shared>> sh;
+    for (int x = 0; x < tiles; ++x) sh.emplace_back(new tile_shared(kW));
+    std::vector<std::thread> th;
+    for (int x = 0; x < tiles; ++x) {
+      for (int l = 0; l < kW; ++l) {
+        th.emplace_back([&, x, l] {
+          mvbt::emu::sm = (uint32_t)x;
+          emu_tile tile{l, kW, sh[x].get()};
+          mvbt::finger<kW> f;
+          const uint32_t E = v.versioned ? v.current_epoch() : 0u;
+          const uint64_t b = (uint64_t)x * per, e = std::min<uint64_t>(n, b + per);
+          for (uint64_t i = b; i < e; ++i) {
+            const uint32_t k = keys[i];
+            if (kind == 0) {
+              const uint32_t r = v.cooperative_find<kW>(k, tile, ts, true, f.start_for(k, tile), &f);
+              if (tile.thread_rank() == 0) out[pos[i]] = r;
+            } else if (kind == 1) {
+              uint2* o = pairs ? reinterpret_cast<uint2*>(pairs) + pos[i] * (uint64_t)avg_len : nullptr;
+              const uint32_t c = v.cooperative_range_query<kW>(k, arg[pos[i]], tile, ts, o, avg_len, true,
+                                                               f.start_for(k, tile), &f);
+              if (out && tile.thread_rank() == 0) out[pos[i]] = c;
+            } else if (kind == 2) {
+              if (i + 1 < n && keys[i + 1] == k) continue;
+              v.insert_in_run<kW>(k, arg[pos[i]], tile, E, f);
+            } else {
+              v.erase_in_run<kW>(k, tile, E, f);
+            }
+          }
+        });
+      }
+    }
+    for (auto& y : th) y.join();
+  });
+}
+
 // One run mixing finds of the newest state and erases (the plain tree's concurrent_find_erase).
 void emu_find_erase(void* h, const uint32_t* fkeys, uint32_t* out, uint64_t n_find,
                     const uint32_t* ekeys, uint64_t n_erase, int tiles, int W) {

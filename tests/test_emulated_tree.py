@@ -174,3 +174,47 @@ def test_emulated_mixed_batches_match_oracle(mode, w):
     assert t.errors == 0
     assert np.array_equal(r, er) and np.array_equal(o, eo)
     assert t.validate()["violations"] == 0
+
+
+@pytest.mark.parametrize("w", [8, 16])
+def test_emulated_sorted_runs_match_oracle(w):
+    """The sorted batch front-end's device code (per-tile runs of sorted keys, each op starting
+    from the deepest covering node of the previous op's path): inserts into a growing tree with
+    repeated keys (the last occurrence wins), updates after a snapshot, erases, and finds and
+    range queries at both snapshots, against the oracle."""
+    from emu import EmuTree
+    import workload as wl
+    import oracle
+    seed, n0 = 11, 4000
+    keys = wl.distinct_keys(seed, 0, n0)
+    vals = wl.values_for(keys, seed)
+    rng = np.random.default_rng(seed)
+    dup = rng.choice(n0, 300, replace=False)
+    ins_k = np.concatenate([keys, keys[dup]])          # 300 keys appear twice
+    ins_v = np.concatenate([vals, wl.values_for(keys[dup], seed ^ 7)])
+    t = EmuTree(True, capacity=1 << 15, tiles=6, W=w)
+    m = oracle.MVMap(True)
+    t.sorted_run("insert", ins_k, ins_v)
+    m.insert(ins_k, ins_v)  # in order: the second occurrence wins
+    s0 = t.snapshot(); assert s0 == m.take_snapshot()
+    upd = keys[rng.choice(n0, 900, replace=False)]
+    t.sorted_run("insert", upd, wl.values_for(upd, seed ^ 1))
+    m.insert(upd, wl.values_for(upd, seed ^ 1))
+    er = keys[rng.choice(n0, 700, replace=False)]
+    t.sorted_run("erase", er)
+    m.erase(er)
+    assert t.errors == 0
+    s1 = t.snapshot(); assert s1 == m.take_snapshot()
+    q = np.concatenate([keys, wl.distinct_keys(seed, wl.MISS_INDEX_BASE, 500)])
+    q = wl.shuffle(seed, q)
+    lo = wl.uniform_keys(seed + 5, 800)
+    hi = wl.upper_bounds(lo, 16, wl.stride_for(n0))
+    for ts in (s0, s1):
+        assert np.array_equal(t.sorted_run("find", q, ts=ts), m.find(q, ts)), ts
+        pairs, counts = t.sorted_run("range", lo, hi, avg_len=48, ts=ts)
+        ep, ec = m.range_query(lo, hi, 48, ts)
+        assert np.array_equal(counts, ec), ts
+        mask = np.arange(48)[None, :] < np.minimum(ec, 48)[:, None]
+        assert np.array_equal(pairs[mask], ep[mask]), ts
+    rep = t.validate()
+    assert rep["violations"] == 0 and rep["locked_nodes"] == 0 and rep["keys"] == m.size()
