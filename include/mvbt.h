@@ -135,7 +135,12 @@ int mvbt_destroy(mvbt_tree* tree);
 int mvbt_set_frontend(mvbt_tree* tree, uint32_t frontend);
 
 /* Upserts n pairs. in_place selects the reference's ViB (1) or VoB (0) insert; both keep every
- * version an older snapshot can read, so results are identical; blink trees ignore it.
+ * version an older snapshot can read, so results are identical; blink trees ignore it. With the
+ * sorted front-end (AUTO or SORTED), an insert of at least 4096 pairs into a pristine tree (created
+ * by mvbt_create, with no write and no snapshot since) is a bulk load: the sorted pairs, each
+ * key's last occurrence, are built bottom up into nodes 10 of 13 pairs full, in the write epoch
+ * of the call, asynchronously like any insert; the contents are those of the pairs upserted in
+ * order.
  * Replaces: gpu_blink_tree::insert (include/gpu_blink_tree.hpp:218-225),
  * gpu_versioned_btree::insert(..., in_place) (include/gpu_versioned_blink_tree.hpp:106-142). */
 int mvbt_insert(mvbt_tree* tree, const uint32_t* keys, const uint32_t* values, uint32_t n,
@@ -240,7 +245,8 @@ int mvbt_reclaim(mvbt_tree* tree, uint32_t min_live_snapshot, void* stream);
  * [6..21] errors per raising site 0..15, [22] locked approaches restarted unlocked, [23] nodes
  * freed by mvbt_reclaim, [24] freed nodes waiting for reuse, [25] nodes handed out again, [26]
  * copies the full retire log could not record (never freed), [27..42] errors per raising site
- * 16..31 (16: rejected batch offsets of mvbt_batch_run_noalloc). Writes min(n, 43) values. */
+ * 16..31 (16: rejected batch offsets of mvbt_batch_run_noalloc; 17: a bulk load into a pristine
+ * tree that did not fit the pool, which leaves the tree empty). Writes min(n, 43) values. */
 int mvbt_stats(mvbt_tree* tree, uint64_t* out, uint32_t n);
 
 /* Device view for user kernels calling the cooperative_* device API. */

@@ -179,7 +179,8 @@ struct control_block {
   unsigned long long stat_max_steps;  // longest unlocked descent of a writer (node visits)
   unsigned long long stat_restarts;   // locked approaches abandoned for an unlocked re-approach
   uint32_t err_site[32];              // errors per raising site (diagnostics; 16 = the
-                                      // offsets check of mvbt_batch_run_noalloc)
+                                      // offsets check of mvbt_batch_run_noalloc, 17 = a
+                                      // bulk load that did not fit the pool)
   unsigned long long sm_pool[kMaxSmSlots];  // per-SM chunk cursor: (base << 32) | used
   // Reclamation of version copies (off when reclaim_cap == 0). The retire log holds the index of
   // every copy made since the last reclaim pass, the free ring the nodes a pass freed; allocation

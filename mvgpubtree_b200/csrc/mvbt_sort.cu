@@ -240,6 +240,17 @@ uint64_t scratch_words(uint32_t n) {
   return counts + sums + 64;
 }
 
+uint64_t scan_scratch_words(uint64_t n) { return (n + kScanChunk - 1) / kScanChunk + 64; }
+
+int exclusive_scan(uint32_t* a, uint64_t n, uint32_t* sums, cudaStream_t s) {
+  if (n == 0) return 0;
+  const uint32_t chunks = (uint32_t)((n + kScanChunk - 1) / kScanChunk);
+  k_scan_reduce<<<chunks, kScanThreads, 0, s>>>(a, n, sums);
+  k_scan_top<<<1, kScanThreads, 0, s>>>(sums, chunks);
+  k_scan_down<<<chunks, kScanThreads, 0, s>>>(a, n, sums);
+  return launch_error() ? 2 : 0;
+}
+
 int sort_pairs(const uint32_t* keys, uint32_t n, int low_bit, uint32_t* k_out, uint32_t* v_out, uint32_t* k_tmp,
                uint32_t* v_tmp, uint32_t* scratch, cudaStream_t s) {
   if (n == 0) return 0;

@@ -18,4 +18,9 @@ uint64_t scratch_words(uint32_t n);
 int sort_pairs(const uint32_t* keys, uint32_t n, int low_bit, uint32_t* k_out, uint32_t* v_out, uint32_t* k_tmp,
                uint32_t* v_tmp, uint32_t* scratch, cudaStream_t s);
 
+// Exclusive prefix sum of a[0, n) in place (uint32, total < 2^32); sums holds
+// scan_scratch_words(n). Stream-ordered; returns 0, or non-zero if a launch failed.
+uint64_t scan_scratch_words(uint64_t n);
+int exclusive_scan(uint32_t* a, uint64_t n, uint32_t* sums, cudaStream_t s);
+
 }  // namespace mvbt_sort

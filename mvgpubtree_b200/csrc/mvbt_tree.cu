@@ -41,6 +41,9 @@ struct mvbt_tree {
   uint32_t max_blocks;
   uint32_t wait_ms;
   uint32_t frontend = MVBT_FRONTEND_AUTO;  // batch front-end of the bulk calls (MVBT_FRONTEND_*)
+  // Nothing has been written to the tree and no snapshot taken since mvbt_create (only the
+  // tombstone {0, 0} in epoch 0): a large sorted insert is then a bottom-up bulk load.
+  bool pristine = false;
   // Upper bound on the keys ever written into the tree (host-side, by the calls that write):
   // leaves are never merged, so it bounds the leaf count from above too. Bulk inserts into a tree
   // that is small against the batch are split by it (insert_launches).
@@ -430,6 +433,7 @@ int sort_pool(int dev, cudaMemPool_t* out) {
 struct sorted_ops {
   uint32_t* keys = nullptr;
   uint32_t* pos  = nullptr;
+  uint32_t* extra = nullptr;  // extra_words of scratch after the sort's own (64-word aligned)
   void* mem      = nullptr;
   int release(cudaStream_t s) {
     if (mem && cudaFreeAsync(mem, s) != cudaSuccess) return fail(MVBT_ERR_CUDA, "cudaFreeAsync of sort scratch");
@@ -438,11 +442,13 @@ struct sorted_ops {
   }
 };
 
-int sort_ops(mvbt_tree* t, const uint32_t* keys, uint32_t n, int low_bit, cudaStream_t s, sorted_ops* out) {
+int sort_ops(mvbt_tree* t, const uint32_t* keys, uint32_t n, int low_bit, cudaStream_t s, sorted_ops* out,
+             uint64_t extra_words = 0) {
   cudaMemPool_t pool;
   int st = sort_pool(t->device, &pool);
   if (st) return st;
-  const uint64_t words = 4ull * n + mvbt_sort::scratch_words(n);
+  const uint64_t sort_words = 4ull * n + ((mvbt_sort::scratch_words(n) + 63) & ~63ull);
+  const uint64_t words      = sort_words + extra_words;
   void* mem            = nullptr;
   if (cudaMallocFromPoolAsync(&mem, words * 4, pool, s) != cudaSuccess) {
     cudaGetLastError();
@@ -452,6 +458,7 @@ int sort_ops(mvbt_tree* t, const uint32_t* keys, uint32_t n, int low_bit, cudaSt
   out->mem    = mem;
   out->keys   = w;
   out->pos    = w + n;
+  out->extra  = extra_words ? w + sort_words : nullptr;
   if (mvbt_sort::sort_pairs(keys, n, low_bit, w, w + n, w + 2ull * n, w + 3ull * n, w + 4ull * n, s)) {
     out->release(s);
     return fail(MVBT_ERR_CUDA, std::string("sort launch: ") + cudaGetErrorString(cudaGetLastError()));
@@ -596,6 +603,7 @@ int mvbt_create(int kind, const mvbt_config* cfg_in, mvbt_tree** out) {
     mvbt_destroy(t);
     return fail(MVBT_ERR_CUDA, std::string("init: ") + cudaGetErrorString(e));
   }
+  t->pristine = true;
   *out = t;
   return MVBT_OK;
 }
@@ -625,14 +633,9 @@ int mvbt_get_info(mvbt_tree* t, int* kind, int* tile_width, int* device) {
 // ---- bulk build from sorted pairs ----
 // Entry e of the built tree: the tombstone {0, 0} first unless the input starts with key 0 (its
 // value then replaces the tombstone's), then the input pairs in order.
-struct bulk_input {
-  const uint32_t* keys;
-  const uint32_t* values;
-  uint32_t off;  // 1: entry 0 is the tombstone; 0: the input holds key 0
-  uint64_t m;    // entries
-  __device__ uint32_t key(uint64_t e) const { return (off && e == 0) ? 0u : keys[e - off]; }
-  __device__ uint32_t value(uint64_t e) const { return (off && e == 0) ? 0u : values[e - off]; }
-};
+// Bottom-up build of a tree from sorted unique pairs, shared by mvbt_bulk_build and by inserts into
+// a pristine tree. The plan lives in device memory, so a build whose entry count is only known on
+// the device (after the sorted front-end dropped repeated keys) needs no host round trip.
 struct bulk_levels {
   uint32_t n;                 // levels, leaves = level 0
   uint32_t fill;              // pairs per leaf = children per interior node
@@ -640,6 +643,59 @@ struct bulk_levels {
   uint64_t count[mvbt::kMaxLevels];  // nodes of each level
   uint64_t span[mvbt::kMaxLevels];   // entries under one node of each level (fill^(level+1), saturated)
 };
+struct bulk_plan {
+  bulk_levels L;
+  const uint32_t* keys;    // sorted strictly increasing
+  const uint32_t* values;
+  uint64_t m;              // entries: the input, plus the tombstone {0, 0} first when off = 1
+  uint64_t total;          // nodes below the anchor; 0 = build nothing
+  uint32_t off;            // 1: entry 0 is the tombstone; 0: the input holds key 0
+  uint32_t status;         // 0 ok, 1 too tall, 2 pool too small
+  __device__ uint32_t key(uint64_t e) const { return (off && e == 0) ? 0u : keys[e - off]; }
+  __device__ uint32_t value(uint64_t e) const { return (off && e == 0) ? 0u : values[e - off]; }
+};
+
+// Level layout of a plan whose m and L.fill are set; leaves total = 0 with a status on failure.
+__host__ __device__ inline void plan_levels(bulk_plan& P, uint64_t capacity) {
+  const uint32_t fill = P.L.fill;
+  P.L.n   = 0;
+  P.total = 0;
+  uint64_t count = (P.m + fill - 1) / fill, base = 1, span = fill, total = 0;
+  for (;;) {
+    if (P.L.n >= (uint32_t)mvbt::kMaxLevels - 1) {
+      P.status = 1;
+      P.L.n    = 0;
+      return;
+    }
+    P.L.base[P.L.n]  = base;
+    P.L.count[P.L.n] = count;
+    P.L.span[P.L.n]  = span;
+    ++P.L.n;
+    base += count;
+    total += count;
+    if (count == 1) break;
+    count = (count + fill - 1) / fill;
+    span  = span > (~0ull) / fill ? ~0ull : span * fill;
+  }
+  if (1 + total > capacity) {
+    P.status = 2;
+    P.L.n    = 0;
+    return;
+  }
+  P.status = 0;
+  P.total  = total;
+}
+
+// Upper bound of plan.total for m entries (the grid of k_bulk_build).
+inline uint64_t bulk_nodes_bound(uint64_t m, uint32_t fill) {
+  uint64_t total = 0, count = (m + fill - 1) / fill;
+  for (int l = 0; l < mvbt::kMaxLevels; ++l) {
+    total += count;
+    if (count <= 1) break;
+    count = (count + fill - 1) / fill;
+  }
+  return total;
+}
 
 // Sorted strictly increasing, no 0xFFFFFFFF: otherwise sets *bad.
 __global__ void k_bulk_check(const uint32_t* keys, uint64_t n, uint32_t* bad) {
@@ -650,32 +706,36 @@ __global__ void k_bulk_check(const uint32_t* keys, uint64_t n, uint32_t* bad) {
 }
 
 // One warp per node, lane w writes word w: pairs 0..12, then {low, mod}, {high, link}, {ts, level|older}.
-__global__ void k_bulk_build(uint32_t* pool, bulk_input in, bulk_levels L, uint64_t total) {
-  const uint32_t w                = threadIdx.x & 31u;
-  const uint64_t warps            = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-  for (uint64_t g = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; g < total; g += warps) {
+__global__ void k_bulk_build(uint32_t* pool, const bulk_plan* __restrict__ plan) {
+  __shared__ bulk_plan P;
+  if (threadIdx.x == 0) P = *plan;
+  __syncthreads();
+  const bulk_levels& L = P.L;
+  const uint32_t w     = threadIdx.x & 31u;
+  const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t g = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; g < P.total; g += warps) {
     uint32_t l = 0;
     while (l + 1 < L.n && g >= L.base[l + 1] - L.base[0]) ++l;
     const uint64_t j     = g - (L.base[l] - L.base[0]);
     const uint64_t first = j * L.span[l];                     // first entry under this node
     const uint64_t child_span = l ? L.span[l - 1] : 1;        // entries under one child (leaf: 1)
-    uint64_t items = l ? L.count[l - 1] - j * L.fill : in.m - first;  // children or entries left
+    uint64_t items = l ? L.count[l - 1] - j * L.fill : P.m - first;  // children or entries left
     if (items > L.fill) items = L.fill;
     uint32_t v = mvbt::kEmptyKey;
     if (w < 2 * mvbt::kDataPairs) {
       const uint64_t p = w >> 1;
       if (p < items) {
         const uint64_t e = first + p * child_span;
-        if (l == 0) v = (w & 1) ? in.value(e) : in.key(e);
-        else v = (w & 1) ? (uint32_t)(L.base[l - 1] + j * L.fill + p) : in.key(e);
+        if (l == 0) v = (w & 1) ? P.value(e) : P.key(e);
+        else v = (w & 1) ? (uint32_t)(L.base[l - 1] + j * L.fill + p) : P.key(e);
       }
     } else if (w == 26) {
-      v = in.key(first);
+      v = P.key(first);
     } else if (w == 27) {
       v = 0;  // modification count
     } else if (w == 28) {
       const uint64_t next = first + L.span[l];
-      v = (j + 1 < L.count[l] && next < in.m) ? in.key(next) : mvbt::kEmptyKey;
+      v = (j + 1 < L.count[l] && next < P.m) ? P.key(next) : mvbt::kEmptyKey;
     } else if (w == 29) {
       v = (j + 1 < L.count[l]) ? (uint32_t)(L.base[l] + j + 1) : mvbt::kNone;
     } else if (w == 30) {
@@ -687,10 +747,20 @@ __global__ void k_bulk_build(uint32_t* pool, bulk_input in, bulk_levels L, uint6
   }
 }
 
-// The anchor {0 -> top}, one level above the top; the bump pointer past the built nodes.
-__global__ void k_bulk_anchor(uint32_t* pool, control_block* c, uint32_t top, uint32_t top_level, uint32_t bump) {
+// The anchor {0 -> top}, one level above the top; the bump pointer past the built nodes. A plan
+// that failed leaves the tree as it was and records the failure in the error bits.
+__global__ void k_bulk_anchor(uint32_t* pool, control_block* c, const bulk_plan* __restrict__ plan) {
   const uint32_t w = threadIdx.x;
   if (w >= 32) return;
+  if (plan->total == 0) {
+    if (w == 0 && plan->status) {
+      atomicOr(&c->error, plan->status == 2 ? mvbt::kErrPoolExhausted : mvbt::kErrCorrupt);
+      atomicAdd(&c->err_site[17], 1u);
+    }
+    return;
+  }
+  const uint32_t top_level = plan->L.n - 1;
+  const uint32_t top       = (uint32_t)plan->L.base[top_level];
   uint32_t v = mvbt::kEmptyKey;
   if (w == 0) v = 0;
   else if (w == 1) v = top;
@@ -698,7 +768,42 @@ __global__ void k_bulk_anchor(uint32_t* pool, control_block* c, uint32_t top, ui
   else if (w == 29) v = mvbt::kNone;
   else if (w == 31) v = ((top_level + 1) << 28) | mvbt::kNone;
   pool[w] = v;
-  if (w == 0) c->bump = bump;
+  if (w == 0) c->bump = (uint32_t)(1 + plan->total);
+}
+
+// ---- insert into a pristine tree: a bulk load of the sorted call ----
+// keep[i] = 1 for the last occurrence of each key (the one an in-order upsert leaves), 0 for an
+// earlier occurrence and for the reserved key 0xFFFFFFFF (which insert ignores).
+__global__ void k_keep_flags(const uint32_t* __restrict__ skeys, uint64_t n, uint32_t* __restrict__ keep) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    keep[i] = (skeys[i] != mvbt::kEmptyKey && !(i + 1 < n && skeys[i + 1] == skeys[i])) ? 1u : 0u;
+}
+// After the exclusive scan of keep (at[i] = output position): the kept pairs, compacted.
+__global__ void k_keep_compact(const uint32_t* __restrict__ skeys, const uint32_t* __restrict__ spos,
+                               const uint32_t* __restrict__ values, const uint32_t* __restrict__ at, uint64_t n,
+                               uint32_t* __restrict__ ck, uint32_t* __restrict__ cv) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t k = skeys[i];
+    if (k != mvbt::kEmptyKey && !(i + 1 < n && skeys[i + 1] == k)) {
+      ck[at[i]] = k;
+      cv[at[i]] = values[spos[i]];
+    }
+  }
+}
+// One thread: the plan for the compacted pairs (their count is at[n - 1] + keep(n - 1)).
+__global__ void k_bulk_plan_kept(const uint32_t* __restrict__ skeys, const uint32_t* __restrict__ at, uint64_t n,
+                                 const uint32_t* ck, const uint32_t* cv, uint32_t fill, uint64_t capacity,
+                                 bulk_plan* plan) {
+  const uint32_t last = skeys[n - 1];
+  const uint64_t kept = (uint64_t)at[n - 1] + (last != mvbt::kEmptyKey ? 1u : 0u);
+  bulk_plan P;
+  P.keys   = ck;
+  P.values = cv;
+  P.off    = (kept && ck[0] == 0u) ? 0u : 1u;  // key 0 in the call replaces the tombstone's value
+  P.m      = kept + P.off;
+  P.L.fill = fill;
+  plan_levels(P, capacity);
+  *plan = P;
 }
 
 int mvbt_bulk_build(mvbt_tree* t, const uint32_t* keys, const uint32_t* values, uint64_t n, uint32_t fill,
@@ -723,29 +828,31 @@ int mvbt_bulk_build(mvbt_tree* t, const uint32_t* keys, const uint32_t* values, 
   MVBT_CUDA_TRY(cudaMemcpyAsync(t->h_word, t->d_words, 4, cudaMemcpyDeviceToHost, s));
   MVBT_CUDA_TRY(cudaStreamSynchronize(s));
   if (*t->h_word) return fail(MVBT_ERR_BAD_ARG, "bulk build needs keys sorted strictly increasing, without 0xFFFFFFFF");
-  bulk_input in{keys, values, first_key == 0 ? 0u : 1u, n + (first_key == 0 ? 0 : 1)};
-  bulk_levels L{};
-  L.fill = fill;
-  uint64_t count = (in.m + fill - 1) / fill, base = 1, span = fill, total = 0;
-  for (;;) {
-    if (L.n >= (uint32_t)mvbt::kMaxLevels - 1) return fail(MVBT_ERR_BAD_ARG, "bulk build: tree too tall");
-    L.base[L.n]  = base;
-    L.count[L.n] = count;
-    L.span[L.n]  = span;
-    ++L.n;
-    base += count;
-    total += count;
-    if (count == 1) break;
-    count = (count + fill - 1) / fill;
-    span  = span > (~0ull) / fill ? ~0ull : span * fill;
-  }
-  if (1 + total > t->capacity) return fail(MVBT_ERR_POOL_EXHAUSTED, "bulk build: the pool is too small");
-  const uint64_t threads = total * 32;
+  bulk_plan P;
+  P.keys   = keys;
+  P.values = values;
+  P.off    = first_key == 0 ? 0u : 1u;
+  P.m      = n + P.off;
+  P.L.fill = fill;
+  plan_levels(P, t->capacity);
+  if (P.status == 1) return fail(MVBT_ERR_BAD_ARG, "bulk build: tree too tall");
+  if (P.status == 2) return fail(MVBT_ERR_POOL_EXHAUSTED, "bulk build: the pool is too small");
+  cudaMemPool_t pool;
+  int st = sort_pool(t->device, &pool);
+  if (st) return st;
+  bulk_plan* dplan = nullptr;
+  MVBT_CUDA_TRY(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&dplan), sizeof(bulk_plan), pool, s));
+  MVBT_CUDA_TRY(cudaMemcpyAsync(dplan, &P, sizeof(bulk_plan), cudaMemcpyHostToDevice, s));  // staged: P may go
+  const uint64_t threads = P.total * 32;
   const unsigned grid    = (unsigned)std::min<uint64_t>((threads + 255) / 256, (uint64_t)t->num_sms * 64);
-  k_bulk_build<<<grid, 256, 0, s>>>(t->pool, in, L, total);
-  k_bulk_anchor<<<1, 32, 0, s>>>(t->pool, t->ctl, (uint32_t)L.base[L.n - 1], L.n - 1, (uint32_t)(1 + total));
+  k_bulk_build<<<grid, 256, 0, s>>>(t->pool, dplan);
+  k_bulk_anchor<<<1, 32, 0, s>>>(t->pool, t->ctl, dplan);
+  st = check_launch();
+  MVBT_CUDA_TRY(cudaFreeAsync(dplan, s));
+  t->pristine = false;
+  if (st) return st;
   t->grown += n;
-  return check_launch();
+  return MVBT_OK;
 }
 
 // ---- copies of a tree: clone on the device, image files for checkpoints ----
@@ -812,7 +919,8 @@ int mvbt_clone(mvbt_tree* src, mvbt_tree** out) {
     mvbt_destroy(t);
     return st;
   }
-  t->grown = src->grown;
+  t->grown    = src->grown;
+  t->pristine = false;
   *out = t;
   return MVBT_OK;
 }
@@ -931,10 +1039,43 @@ int mvbt_load(const char* path, int device, mvbt_tree** out) {
     mvbt_destroy(t);
     return st;
   }
-  t->grown = std::max<uint64_t>(1, (uint64_t)c.bump * 16);  // at most 16 keys per node
+  t->grown    = std::max<uint64_t>(1, (uint64_t)c.bump * 16);  // at most 16 keys per node
+  t->pristine = false;
   *out = t;
   return MVBT_OK;
 }
+
+namespace {
+// Leaves and interior nodes of a bulk load hold 10 of 13 pairs: later inserts split a leaf after
+// three more keys, and a tree built by inserts averages about 9.7.
+constexpr uint32_t kLoadFill = 10;
+constexpr uint32_t kLoadMin  = 1u << 12;  // smaller inserts into a pristine tree go key by key
+
+uint64_t bulk_load_extra_words(uint32_t n) {
+  return (uint64_t)n + ((mvbt_sort::scan_scratch_words(n) + 63) & ~63ull) + (sizeof(bulk_plan) + 255) / 4;
+}
+
+// Insert of a sorted call into a pristine tree: the last occurrence of every key, compacted, built
+// bottom up (k_bulk_build) in place of the tombstone leaf. Stream-ordered, no host round trip: the
+// entry count and the level plan are computed on the device.
+int bulk_load_sorted(mvbt_tree* t, const sorted_ops& so, const uint32_t* values, uint32_t n, cudaStream_t s) {
+  uint32_t* ck   = so.keys + 2ull * n;  // the sort's ping-pong buffers are free again
+  uint32_t* cv   = so.keys + 3ull * n;
+  uint32_t* keep = so.extra;
+  uint32_t* sums = so.extra + n;
+  auto* plan     = reinterpret_cast<bulk_plan*>(so.extra + n + ((mvbt_sort::scan_scratch_words(n) + 63) & ~63ull));
+  const unsigned grid = (unsigned)std::min<uint64_t>(((uint64_t)n + 255) / 256, (uint64_t)t->num_sms * 16);
+  k_keep_flags<<<grid, 256, 0, s>>>(so.keys, n, keep);
+  if (mvbt_sort::exclusive_scan(keep, n, sums, s)) return check_launch();
+  k_keep_compact<<<grid, 256, 0, s>>>(so.keys, so.pos, values, keep, n, ck, cv);
+  k_bulk_plan_kept<<<1, 1, 0, s>>>(so.keys, keep, n, ck, cv, kLoadFill, t->capacity, plan);
+  const uint64_t threads = bulk_nodes_bound((uint64_t)n + 1, kLoadFill) * 32;
+  k_bulk_build<<<(unsigned)std::min<uint64_t>((threads + 255) / 256, (uint64_t)t->num_sms * 64), 256, 0, s>>>(t->pool, plan);
+  k_bulk_anchor<<<1, 32, 0, s>>>(t->pool, t->ctl, plan);
+  t->grown += n;
+  return check_launch();
+}
+}  // namespace
 
 int mvbt_insert(mvbt_tree* t, const uint32_t* keys, const uint32_t* values, uint32_t n, void* stream,
                 int in_place) {
@@ -942,12 +1083,17 @@ int mvbt_insert(mvbt_tree* t, const uint32_t* keys, const uint32_t* values, uint
   if (!t || (n && (!keys || !values))) return fail(MVBT_ERR_BAD_ARG, "null argument");
   if (n == 0) return MVBT_OK;
   cudaStream_t s = as_stream(stream);
-  if (use_sorted(t, n)) {
+  const bool load = t->pristine && n >= kLoadMin && t->frontend != MVBT_FRONTEND_UNSORTED;
+  t->pristine     = false;
+  if (load || use_sorted(t, n)) {
     sorted_ops so;
-    int st = sort_ops(t, keys, n, 0, s, &so);
+    int st = sort_ops(t, keys, n, 0, s, &so, load ? bulk_load_extra_words(n) : 0);
     if (st) return st;
-    st = t->tile_width == 8 ? insert_sorted_launches<8>(t, so, values, n, s)
-                            : insert_sorted_launches<16>(t, so, values, n, s);
+    if (load)
+      st = bulk_load_sorted(t, so, values, n, s);
+    else
+      st = t->tile_width == 8 ? insert_sorted_launches<8>(t, so, values, n, s)
+                              : insert_sorted_launches<16>(t, so, values, n, s);
     const int rs = so.release(s);
     return st ? st : rs;
   }
@@ -990,6 +1136,7 @@ int mvbt_find(mvbt_tree* t, const uint32_t* keys, uint32_t* values, uint32_t n, 
 int mvbt_erase(mvbt_tree* t, const uint32_t* keys, uint32_t n, void* stream, int concurrent) {
   (void)concurrent;  // writers always use coherent loads
   if (!t || (n && !keys)) return fail(MVBT_ERR_BAD_ARG, "null argument");
+  t->pristine = false;
   if (n == 0) return MVBT_OK;
   cudaStream_t s = as_stream(stream);
   if (use_sorted(t, n)) {
@@ -1056,12 +1203,14 @@ int mvbt_set_frontend(mvbt_tree* t, uint32_t frontend) {
 
 int mvbt_take_snapshot_async(mvbt_tree* t, void* stream, uint32_t* d_out) {
   if (!t || !d_out) return fail(MVBT_ERR_BAD_ARG, "null argument");
+  t->pristine = false;
   k_snapshot<<<1, 32, 0, as_stream(stream)>>>(t->ctl, d_out);
   return check_launch();
 }
 
 int mvbt_take_snapshot(mvbt_tree* t, void* stream, uint32_t* snapshot_out) {
   if (!t || !snapshot_out) return fail(MVBT_ERR_BAD_ARG, "null argument");
+  t->pristine = false;
   if (t->kind != MVBT_KIND_VERSIONED) return fail(MVBT_ERR_NOT_SUPPORTED, "snapshots need a versioned tree");
   cudaStream_t s = as_stream(stream);
   k_snapshot<<<1, 32, 0, s>>>(t->ctl, t->d_words);
@@ -1081,6 +1230,7 @@ int mvbt_concurrent_insert_range(mvbt_tree* t, const uint32_t* keys, const uint3
     return fail(MVBT_ERR_BAD_ARG, "null argument");
   uint64_t total = (uint64_t)n_ins + n_rq;
   if (total == 0) return MVBT_OK;
+  t->pristine = false;
   cudaStream_t s = as_stream(stream);
   if (t->kind == MVBT_KIND_VERSIONED) {
     k_snapshot<<<1, 32, 0, s>>>(t->ctl, t->d_words);
@@ -1104,6 +1254,7 @@ int mvbt_concurrent_find_erase(mvbt_tree* t, const uint32_t* fkeys, uint32_t* fr
   if (!t || (n_find && (!fkeys || !fres)) || (n_erase && !ekeys)) return fail(MVBT_ERR_BAD_ARG, "null argument");
   uint64_t total = (uint64_t)n_find + n_erase;
   if (total == 0) return MVBT_OK;
+  t->pristine = false;
   cudaStream_t s = as_stream(stream);
   if (t->kind == MVBT_KIND_VERSIONED) {
     k_snapshot<<<1, 32, 0, s>>>(t->ctl, t->d_words);
@@ -1193,7 +1344,10 @@ int mvbt_internal_view(mvbt_tree* t, device_tree* view, int* tile_width, int* bl
 void mvbt_internal_set_error(const char* msg) { g_last_error = msg ? msg : ""; }
 
 void mvbt_internal_note_growth(mvbt_tree* t, uint64_t keys) {
-  if (t) t->grown += keys;
+  if (t) {
+    t->grown += keys;
+    t->pristine = false;  // batches and serving write and take snapshots
+  }
 }
 
 int mvbt_stats(mvbt_tree* t, uint64_t* out, uint32_t n) {

@@ -155,3 +155,68 @@ def test_auto_frontend_gives_the_same_results_as_both(torch):
         assert t.check_errors() == 0
         t.close()
     assert np.array_equal(outs[0], outs[1]) and np.array_equal(outs[1], outs[2])
+
+
+@pytest.mark.parametrize("kind", ["versioned", "blink"])
+def test_insert_into_a_pristine_tree_is_a_bulk_load_with_the_same_contents(torch, kind):
+    """A large insert into a tree nothing has written yet is built bottom up from the sorted call:
+    the same contents as the pairs upserted in order (repeated keys: the last occurrence wins; key 0
+    replaces the tombstone's value), a valid structure, snapshots and later writes behaving as on
+    an insert-built tree."""
+    import mvgpubtree_b200 as mv
+    import oracle
+    import workload as wl
+    seed, n0 = 59, 1 << 20
+    keys = wl.distinct_keys(seed, 0, n0)
+    vals = wl.values_for(keys, seed)
+    rng = np.random.default_rng(seed)
+    dup = rng.choice(n0, 5000, replace=False)
+    ik = np.concatenate([keys, keys[dup], np.array([0, 0xFFFFFFFF], np.uint32)])
+    iv = np.concatenate([vals, wl.values_for(keys[dup], seed ^ 3), np.array([77, 5], np.uint32)])
+    perm = rng.permutation(ik.size)
+    ik, iv = ik[perm], iv[perm]
+    cls = mv.gpu_versioned_btree if kind == "versioned" else mv.gpu_blink_tree
+    t = cls(pool_bytes=1 << 30)
+    m = oracle.MVMap(kind == "versioned")
+    t.insert(dev(torch, ik), dev(torch, iv))
+    m.insert(ik[ik != 0xFFFFFFFF], iv[ik != 0xFFFFFFFF])
+    assert t.check_errors() == 0
+    rep = t.validate_tree_structure()
+    assert rep["violations"] == 0 and rep["locked_nodes"] == 0 and rep["keys"] == m.size()
+    k_all, v_all = m.dump()
+    q = np.concatenate([k_all, wl.distinct_keys(seed, wl.MISS_INDEX_BASE, 1 << 16)])
+    out = torch.empty(q.size, dtype=torch.int32, device="cuda")
+    t.find(dev(torch, q), out)
+    assert np.array_equal(host(out), m.find(q))
+    if kind == "versioned":  # a snapshot, then updates, erases and inserts on the loaded tree
+        s0 = t.take_snapshot(); assert s0 == m.take_snapshot()
+        upd = wl.shuffle(seed + 1, keys)[: n0 // 8]
+        t.insert(dev(torch, upd), dev(torch, wl.values_for(upd, seed ^ 1))); m.insert(upd, wl.values_for(upd, seed ^ 1))
+        er = wl.shuffle(seed + 2, keys)[: n0 // 8]
+        t.erase(dev(torch, er)); m.erase(er)
+        new = wl.distinct_keys(seed, n0, n0 // 4)
+        t.insert(dev(torch, new), dev(torch, wl.values_for(new, seed))); m.insert(new, wl.values_for(new, seed))
+        s1 = t.take_snapshot(); assert s1 == m.take_snapshot()
+        q2 = np.concatenate([q, new])
+        for ts in (s0, s1):
+            out2 = torch.empty(q2.size, dtype=torch.int32, device="cuda")
+            t.find(dev(torch, q2), out2, timestamp=ts)
+            assert np.array_equal(host(out2), m.find(q2, ts)), ts
+        rep = t.validate_tree_structure()
+        assert rep["violations"] == 0 and rep["keys"] == m.size()
+    assert t.check_errors() == 0
+
+
+def test_bulk_load_reports_a_pool_too_small_and_leaves_the_tree_empty(torch):
+    import mvgpubtree_b200 as mv
+    import workload as wl
+    n = 1 << 20  # needs ~116K nodes; the pool holds 8192
+    keys = wl.distinct_keys(61, 0, n)
+    t = mv.gpu_versioned_btree(pool_bytes=1 << 20)
+    t.insert(dev(torch, keys), dev(torch, wl.values_for(keys, 61)))
+    bits = t.check_errors(raise_on_error=False)
+    assert bits & 1  # MVBT_DEVERR_POOL_EXHAUSTED
+    assert t.stats()["error_sites"].get(17, 0) == 1
+    t.clear_errors()
+    rep = t.validate_tree_structure()
+    assert rep["violations"] == 0 and rep["keys"] == 1  # the tombstone only
