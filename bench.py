@@ -78,8 +78,15 @@ def parse_args():
                     help="keep --tile-width / --blocks-per-sm instead of tuning the launch shape")
     ap.add_argument("--serve-loads", default="10,50,200",
                     help="offered loads (M ops/s) of the serving sessions; empty = no serving run")
-    ap.add_argument("--serve-seconds", type=float, default=0.25,
-                    help="arrival window of each serving session")
+    ap.add_argument("--serve-seconds", type=float, default=4.0,
+                    help="arrival window of each serving session, capped at --serve-max-ops ops of trace")
+    ap.add_argument("--serve-max-ops", type=float, default=50e6,
+                    help="most ops of one serving session's trace (the whole trace and its range "
+                         "output slots are held in pinned host memory)")
+    ap.add_argument("--serve-max-lag", type=int, default=1 << 22,
+                    help="serving admission: most version copies waiting for reclamation")
+    ap.add_argument("--no-reclaim-arm", action="store_true",
+                    help="skip the batched steps with reclamation inside the persistent launch")
     ap.add_argument("--no-configs", action="store_true",
                     help="skip the c1-c3 workloads (plain finds, finds at snapshots, concurrent "
                          "insert + range) reported under \"configs\"")
@@ -345,10 +352,58 @@ def run_ours(args, dist: Dist):
 
     # range counts of the timed steps (for the roofline bytes), read after the timed region
     host_res = [results["batched"][s].cpu().numpy().view(np.uint32) for s in range(W, W + K)]
-    del dsteps, results
     plans["plain"].close()
     trees["plain"].close()
-    del plans["plain"], trees["plain"], range_out["plain"]
+    del plans["plain"], trees["plain"], range_out["plain"], results["plain"]
+    torch.cuda.empty_cache()
+
+    # ---- the same steps with reclamation inside the persistent launch, on a tree created with
+    # reclamation: copies freed while the launch runs and handed out again by the same launch ----
+    reclaim_inside = None
+    if not args.no_reclaim_arm:
+        tr = mv.gpu_versioned_btree(pool_bytes=pool, tile_width=args.tile_width, reclaim=True)
+        tr.insert(dev(init), dev(vals))
+        pr = tr.batch_plan(max_ops, args.batches)
+        if tune:
+            pr.set_launch(tune["tile_width"], tune["blocks_per_sm"])
+        pr.set_reclaim(True)
+        rr = torch.empty(max_ops, dtype=torch.int32, device="cuda")
+        nodes, live_lo, live_hi, mism = [], None, None, 0
+        for s in range(W):
+            pr.run(steps[s].batch_off, *dsteps[s], rr[: steps[s].num_ops], range_out["batched"], mode=mv.BATCH_PERSISTENT)
+            mism += int((rr[: steps[s].num_ops] != results["batched"][s]).sum())
+        tr.check_errors()
+        pr.enable_timing(True)
+        torch.cuda.synchronize()
+        r0e, r1e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        outs_r = [torch.empty(steps[s].num_ops, dtype=torch.int32, device="cuda") for s in range(W, W + K)]
+        r0e.record(stream)
+        for j, s in enumerate(range(W, W + K)):
+            pr.run(steps[s].batch_off, *dsteps[s], outs_r[j], range_out["batched"], mode=mv.BATCH_PERSISTENT)
+        r1e.record(stream)
+        torch.cuda.synchronize()
+        rms = dist.max(r0e.elapsed_time(r1e))
+        pr.enable_timing(False)
+        tr.check_errors()
+        ser = pr.memory_series().astype(np.int64)  # the last timed step, per batch
+        live = ser[:, 1] - ser[:, 2]
+        mism += sum(int((outs_r[j] != results["batched"][s]).sum()) for j, s in enumerate(range(W, W + K)))
+        st = tr.stats()
+        reclaim_inside = {
+            "value": round(ops_all / (rms * 1e-3) / 1e6, 2), "unit": UNIT, "steps": K,
+            "results_identical_to_batched": mism == 0,
+            "nodes_taken_from_pool": int(tr.compute_memory_usage()["nodes_allocated"]),
+            "nodes_taken_without_reclamation": int(trees["batched"].compute_memory_usage()["nodes_allocated"]),
+            "copies_freed": int(st["reclaimed"]), "freed_nodes_reused": int(st["reused"]),
+            "live_nodes_last_step": {"first_batch": int(live[0]), "last_batch": int(live[-1]),
+                                     "min": int(live.min()), "max": int(live.max())},
+            "how": "the batched arm's steps on a tree created with reclamation; copies freed inside "
+                   "each persistent launch once the batches that read them have finished"}
+        outs_r.clear()
+        pr.close()
+        tr.close()
+        del rr
+    del dsteps, results
     torch.cuda.empty_cache()
 
     # ---- e2e: public API with pinned host buffers, CUDA graph replay, two steps in flight ----
@@ -513,6 +568,8 @@ def run_ours(args, dist: Dist):
         "gpu_launches": 5 * K,
         "verified": {"batched_vs_plain": batched_vs_plain},
     }
+    if reclaim_inside is not None:
+        out["reclaim_inside_launch"] = reclaim_inside
     plain = {"value": round(plain_value, 2), "unit": UNIT, "steps": K, "warmup": W,
              "ms_per_step": round(plain_ms / K, 3), "batched_over_plain": round(value / plain_value, 3),
              "same_steps_as_batched": True, "clocks": plain_clk,
@@ -571,16 +628,18 @@ def run_serving(args, seed: int, init, vals, dev) -> dict:
     mean_size = 657.0  # mean of the request-size distribution (lognormal median 256, sigma 1.5)
     per_load = []
     for k, load in enumerate(loads):
-        R = max(16, int(load * 1e6 * args.serve_seconds / mean_size))
+        seconds = min(args.serve_seconds, args.serve_max_ops / (load * 1e6))
+        R = max(16, int(load * 1e6 * seconds / mean_size))
         b, arrival = wl.serving_trace(seed + 11 * (k + 1), 0, R, load, 0, generator=gen)
-        res = {"offered_mops": load, "requests": R, "ops": int(b.num_ops)}
+        res = {"offered_mops": load, "seconds": round(seconds, 3), "requests": R, "ops": int(b.num_ops)}
         for name, t in trees.items():
-            o = t.serve(b, arrival, mode=mv.BATCH_PERSISTENT if name == "batched" else mv.BATCH_PER_LAUNCH,
-                        reclaim_every=8 if name == "batched" else 0)
+            kw = ({"reclaim_in_launch": 1, "max_reclaim_lag": args.serve_max_lag} if name == "batched"
+                  else {})
+            o = t.serve(b, arrival, mode=mv.BATCH_PERSISTENT if name == "batched" else mv.BATCH_PER_LAUNCH, **kw)
             t.check_errors()
             summ = latency_summary(arrival, o["done_ns"], b.num_ops)
-            summ.update({"launches": o["stats"]["launches"], "reclaims": o["stats"]["reclaims"],
-                         "max_waiting": o["stats"]["max_waiting"]})
+            summ.update({k: o["stats"][k] for k in ("launches", "reclaims", "max_waiting", "memory_waits",
+                                                     "max_reclaim_lag", "lag_waits", "nodes_high_water")})
             res[name] = summ
         per_load.append(res)
     st = trees["batched"].stats()
@@ -589,9 +648,10 @@ def run_serving(args, seed: int, init, vals, dev) -> dict:
     gen.close()
     return {"mode": "continuous batching: the requests that arrived while the previous launch ran "
                     "form the next launch, one snapshot per admitted batch (reads at it, writes after), "
-                    "reclaim every 8 launches",
+                    "reclamation inside every launch, admission by free nodes and by reclamation lag",
             "request_size": "lognormal median 256 ops, sigma 1.5, clipped [1, 65536]",
-            "arrivals": "Poisson", "seconds_per_load": args.serve_seconds, "pool_gb": args.pool_gb,
+            "arrivals": "Poisson", "seconds_per_load": "min(serve_seconds, serve_max_ops / load)",
+            "serve_seconds": args.serve_seconds, "serve_max_ops": args.serve_max_ops, "pool_gb": args.pool_gb,
             "per_load": per_load,
             "headline": {"offered_mops": head["offered_mops"], **{k: head["batched"][k] for k in
                          ("achieved_mops", "p50_us", "p99_us", "p999_us")}},

@@ -310,6 +310,26 @@ int mvbt_batch_run(mvbt_batch_plan* plan, uint32_t num_batches, const uint64_t* 
  * (up to 64 runs are kept); mvbt_batch_plan_kernel_times waits for them, writes the kernel times
  * in ms of the runs since the last call (oldest first, at most max) and their number to *n. */
 int mvbt_batch_plan_timing(mvbt_batch_plan* plan, int enable);
+
+/* Reclamation inside the plan's persistent runs (MVBT_BATCH_PERSISTENT and MVBT_BATCH_GRAPH;
+ * config.reclaim trees, else MVBT_ERR_NOT_SUPPORTED). While a run goes on, warps without work
+ * free the version copies that no snapshot of the run reads any more -- those batch b and
+ * earlier made, once batches 0..b have finished their writes and their reads -- together with the
+ * copies made before the run, and append them to the free ring, from which the same run's writes
+ * allocate. min_live_snapshot is the oldest snapshot the caller still reads outside the run, as in
+ * mvbt_reclaim: copies made in later epochs are kept (MVBT_RECLAIM_ALL: none held).
+ * Replaces: the reference's device-side epoch-based reclaimer DEBR_device (retire, leave_qstate,
+ * enter_qstate; include/memory_reclaimer.hpp:146-410), which frees retired nodes about two
+ * epoch advances after retirement whether or not a snapshot still reads them; here the batches'
+ * own completion counters are the announcements, and a held snapshot stays exact. */
+int mvbt_batch_plan_set_reclaim(mvbt_batch_plan* plan, int enable, uint32_t min_live_snapshot);
+
+/* Memory over time of the plan's last persistent run with reclamation on: per batch b (up to
+ * max_batches), 4 values sampled when its writes had finished: the write epoch, nodes ever taken
+ * from the pool (bump pointer), freed nodes waiting in the free ring, and nodes freed so far; live
+ * nodes = bump - waiting. *n = batches written. Waits for the run. Replaces the reference's
+ * per-epoch reclaimer statistics (compute_reclaimer_stats, include/memory_reclaimer.hpp:114-133). */
+int mvbt_batch_plan_memory_series(mvbt_batch_plan* plan, uint64_t* out, uint32_t max_batches, uint32_t* n);
 int mvbt_batch_plan_kernel_times(mvbt_batch_plan* plan, float* ms, uint32_t max, uint32_t* n);
 
 /* Mixed batches for callers that cannot allocate device memory on their call path: a serving
@@ -366,7 +386,13 @@ typedef struct mvbt_serve_config {
   uint32_t nodes_per_write;         /* admission: nodes a write may allocate (0 = 3) */
   uint32_t snapshots;               /* MVBT_SERVE_SNAPSHOT_PER_BATCH (0) or _PER_REQUEST */
   uint64_t reserve_nodes;           /* admission: nodes kept free (0 = 1 << 16) */
-  uint64_t reserved[4];
+  uint32_t reclaim_in_launch;       /* 1: reclamation inside every persistent launch
+                                       (mvbt_batch_plan_set_reclaim; config.reclaim trees) */
+  uint32_t pad0;
+  uint64_t max_reclaim_lag;         /* admission: while more version copies than this wait in the
+                                       retire log (retired, not yet freed), no request is admitted
+                                       until a reclaim pass has run (0 = no limit) */
+  uint64_t reserved[2];
 } mvbt_serve_config;
 
 typedef struct mvbt_serve_stats {
@@ -378,7 +404,10 @@ typedef struct mvbt_serve_stats {
   uint64_t max_waiting;   /* most requests arrived but not yet admitted at one time */
   uint64_t memory_waits;  /* admissions deferred until memory was freed */
   uint64_t max_launch_ops;
-  uint64_t reserved[8];
+  uint64_t max_reclaim_lag;  /* most version copies seen waiting for reclamation after a launch */
+  uint64_t lag_waits;        /* admissions deferred by max_reclaim_lag */
+  uint64_t nodes_high_water; /* most nodes in use (taken from the pool, not free) after a launch */
+  uint64_t reserved[5];
 } mvbt_serve_stats;
 
 void mvbt_serve_config_init(mvbt_serve_config* cfg);

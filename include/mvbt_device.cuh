@@ -146,6 +146,7 @@ constexpr uint32_t kFreeBit    = 0x20000000u;
 constexpr uint32_t kCountMask  = 0x1FFFFFFFu;  // count (live node) or epoch (retired copy)
 constexpr int kModWord         = 27;
 constexpr uint32_t kRingChunk  = 0x80000000u;  // per-SM chunk base: positions in the free ring
+constexpr uint32_t kRingEmpty  = 0xFFFFFFFFu;  // a free-ring slot not written yet (or read already)
 constexpr uint32_t kReclaimAll = 0xFFFFFFFFu;  // reclaim watermark: the current epoch
 constexpr uint32_t kAnchor    = 0;  // fixed entry node: one entry {0 -> top}, level = top + 1
 constexpr uint32_t kFirstLeaf = 1;  // the initial leaf (holds the tombstone {0, 0})
@@ -183,24 +184,28 @@ struct control_block {
                                       // bulk load that did not fit the pool)
   unsigned long long sm_pool[kMaxSmSlots];  // per-SM chunk cursor: (base << 32) | used
   // Reclamation of version copies (off when reclaim_cap == 0). The retire log holds the index of
-  // every copy made since the last reclaim pass, the free ring the nodes a pass freed; allocation
-  // refills a per-SM chunk from the free ring before the bump pointer.
+  // every copy not yet reclaimed, in the order the copies were made (which is epoch order); the
+  // free ring the nodes reclamation freed. Allocation refills a per-SM chunk from the free ring
+  // before the bump pointer. Both run while kernels run: a copy reserves a log position
+  // (retire_tail) and writes it; a reclaimer claims log positions below a limit it knows to be
+  // safe (retire_head), frees the copies, reserves ring positions (free_tail), writes them and
+  // then counts them in free_avail; an allocation takes free_avail first, then ring positions
+  // (free_head), waits for each slot to be written and clears it again (kRingEmpty) as it reads it.
   unsigned long long retire_log;   // device address of uint32_t[reclaim_cap]
-  unsigned long long free_ring;    // device address of uint32_t[reclaim_cap]
+  unsigned long long free_ring;    // device address of uint32_t[ring_cap]
   unsigned long long retire_head, retire_tail;  // log positions (monotonic; slot = pos % cap)
   unsigned long long free_head, free_tail;      // ring positions (monotonic; slot = pos % cap)
+  unsigned long long free_avail;                // ring entries written and not yet taken (signed)
   uint32_t reclaim_cap;     // retire log entries: a power of two >= pool capacity
-  uint32_t rc_pending;      // nodes freed by the running pass
-  uint32_t rc_first_kept;   // first log entry (relative to retire_head) the pass had to keep
+  uint32_t rc_first_kept;   // first log entry (relative to retire_head) a pass had to keep
   uint32_t ring_cap;        // free ring slots: a power of two >= capacity + kMaxSmSlots * chunk
-  unsigned long long stat_reclaimed;    // nodes freed by reclaim passes
+  uint32_t reserved2;
+  unsigned long long stat_reclaimed;    // nodes freed (passes between kernels and reclamation in them)
   unsigned long long stat_log_dropped;  // copies not logged because the log was full (never freed)
-  unsigned long long stat_reused;       // nodes handed out again from the free ring
-  unsigned long long ring_fail;  // first ring position of a failed chunk pop (~0: none)
-  unsigned long long free_mark;  // ring head at the end of the last pass (for stat_reused)
-  // Per-SM shares of the copy and split counts ([slot][0] copies, [slot][1] splits), one 128-B
-  // line per SM slot: the counting atomics of different SMs land on different lines instead of
-  // all on one word. stat_cow / stat_split stay 0; a count is its slots' sum (stat_total).
+  // Per-SM shares of counters, one 128-B line per SM slot ([slot][0] copies, [slot][1] splits,
+  // [slot][2] freed nodes handed out again): the counting atomics of different SMs land on
+  // different lines instead of all on one word. stat_cow / stat_split stay 0; a count is its
+  // slots' sum (stat_total).
   unsigned long long sm_stats[kMaxSmSlots][16];
 };
 
@@ -211,9 +216,9 @@ struct control_block {
 #define MVBT_HD __host__ __device__ __forceinline__
 #endif
 
-// Total of per-SM counter k (0 copies, 1 splits) plus the unsharded field.
+// Total of per-SM counter k (0 copies, 1 splits, 2 freed nodes reused) plus the unsharded field.
 MVBT_HD unsigned long long stat_total(const control_block& c, int k) {
-  unsigned long long s = k == 0 ? c.stat_cow : c.stat_split;
+  unsigned long long s = k == 0 ? c.stat_cow : (k == 1 ? c.stat_split : 0ull);
   for (int i = 0; i < kMaxSmSlots; ++i) s += c.sm_stats[i][k];
   return s;
 }
@@ -268,15 +273,13 @@ MVBT_HD void init_control(control_block& c, uint32_t capacity, uint32_t chunk, u
   c.retire_tail      = 0;
   c.free_head        = 0;
   c.free_tail        = 0;
+  c.free_avail       = 0;
   c.reclaim_cap      = reclaim_cap;
-  c.rc_pending       = 0;
   c.rc_first_kept    = 0xFFFFFFFFu;
   c.ring_cap         = ring_cap;
+  c.reserved2        = 0;
   c.stat_reclaimed   = 0;
   c.stat_log_dropped = 0;
-  c.stat_reused      = 0;
-  c.ring_fail        = ~0ull;
-  c.free_mark        = 0;
 }
 
 // ----------------------------------------------------------------------------------------------
@@ -297,6 +300,7 @@ MVBT_DEV unsigned long long global_ns() {
       .count();
 }
 MVBT_DEV uint32_t ld_relaxed_u32(const uint32_t* p) { return __atomic_load_n(p, __ATOMIC_RELAXED); }
+MVBT_DEV void st_relaxed_u32(uint32_t* p, uint32_t v) { __atomic_store_n(p, v, __ATOMIC_RELAXED); }
 MVBT_DEV unsigned long long ld_relaxed_u64(const unsigned long long* p) {
   return __atomic_load_n(p, __ATOMIC_RELAXED);
 }
@@ -336,6 +340,9 @@ MVBT_DEV unsigned long long ld_relaxed_u64(const unsigned long long* p) {
   unsigned long long r;
   asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(r) : "l"(p) : "memory");
   return r;
+}
+MVBT_DEV void st_relaxed_u32(uint32_t* p, uint32_t v) {
+  asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" : : "l"(p), "r"(v) : "memory");
 }
 
 // Loads this lane's share of a node. strong = L2-coherent relaxed loads (needed while writers
@@ -616,26 +623,82 @@ MVBT_DEV int find_pos(const node_regs<W>& n, uint32_t key, const Tile& t) {
 // The tree view: a plain struct passed to kernels by value.
 // ----------------------------------------------------------------------------------------------
 // ---- allocation and retirement slow paths (free functions: no copy of the tree view) ----
-// Node `used` of the chunk that starts at `base`: consecutive nodes of the bump range, or
-// consecutive free-ring positions (kRingChunk set).
-MVBT_DEV uint32_t chunk_node(const control_block* c, uint32_t base, uint32_t used) {
-  if (!(base & kRingChunk)) return base + used;
-  const uint32_t* ring = reinterpret_cast<const uint32_t*>(c->free_ring);
-  return ring[((unsigned long long)(base & ~kRingChunk) + used) & (c->ring_cap - 1u)];
+// Whether the bounded wait that started at t0 (lane 0's clock) has run past `limit` ns, decided by
+// lane 0 for the whole tile or warp. Every lane of a group that runs warp-synchronous operations
+// inside a wait loop must leave the loop together: a lane that left alone would make the next
+// shuffle or ballot of the others name a lane that no longer takes part.
+template <class Group>
+MVBT_DEV bool wait_expired(unsigned long long t0, unsigned long long limit, const Group& g) {
+  uint32_t late = 0;
+  if (g.thread_rank() == 0) late = global_ns() - t0 > limit ? 1u : 0u;
+  return g.shfl(late, 0) != 0;
 }
-// Takes C consecutive free-ring positions for a chunk (reclamation on and enough freed nodes):
-// one atomic on the ring head. The ring tail only moves between kernels, so positions below it
-// are written. A pop past the tail fails and records its position; every later pop fails too,
-// and the next reclaim pass moves the head back to the first failed position (those entries were
-// never handed out).
-MVBT_DEV bool take_free_chunk(control_block* c, uint32_t C, uint32_t& base) {
-  const unsigned long long h = atomicAdd(&c->free_head, (unsigned long long)C);
-  if (h + C <= c->free_tail) {
-    base = kRingChunk | (uint32_t)(h & (c->ring_cap - 1u));
-    return true;
+
+// Node `used` of the chunk that starts at `base`: consecutive nodes of the bump range, or the node
+// stored at consecutive free-ring positions (kRingChunk set). A ring slot is read once: the reader
+// waits (bounded) for its pusher to have written it and clears it (kRingEmpty) for the ring's next
+// lap. Returns kNone (and records kErrSpinLimit) if the slot stays empty past the wait limit. The
+// ring and the retire log start filled with kRingEmpty (all bits set).
+MVBT_DEV uint32_t chunk_node(control_block* c, uint32_t base, uint32_t used) {
+  if (!(base & kRingChunk)) return base + used;
+  uint32_t* slot = reinterpret_cast<uint32_t*>(c->free_ring) +
+                   (((unsigned long long)(base & ~kRingChunk) + used) & (c->ring_cap - 1u));
+  uint32_t v                  = ld_relaxed_u32(slot);
+  const unsigned long long t0 = v == kRingEmpty ? global_ns() : 0;
+  while (v == kRingEmpty) {
+    if (global_ns() - t0 > c->wait_ns) {
+      atomicOr(&c->error, kErrSpinLimit);
+      atomicAdd(&c->err_site[18], 1u);
+      return kNone;
+    }
+    __nanosleep(64);
+    v = ld_relaxed_u32(slot);
   }
-  atomicMin(&c->ring_fail, h);
-  return false;
+  st_relaxed_u32(slot, kRingEmpty);
+  atomicAdd(&c->sm_stats[sm_id() % kMaxSmSlots][2], 1ull);  // a freed node handed out again
+  return v;
+}
+// Takes C free-ring entries for a chunk: one atomic on free_avail (undone if fewer are there),
+// then one on the ring head for their positions. False: allocate from the bump pointer instead.
+MVBT_DEV bool take_free_chunk(control_block* c, uint32_t C, uint32_t& base) {
+  if ((long long)ld_relaxed_u64(&c->free_avail) < (long long)C) return false;
+  const long long a = (long long)atomicAdd(&c->free_avail, (unsigned long long)(-(long long)C));
+  if (a < (long long)C) {
+    atomicAdd(&c->free_avail, (unsigned long long)C);
+    return false;
+  }
+  const unsigned long long h = atomicAdd(&c->free_head, (unsigned long long)C);
+  base                       = kRingChunk | (uint32_t)(h & (c->ring_cap - 1u));
+  return true;
+}
+// Appends the nodes of the lanes with `freed` set to the free ring (warp-collective, every lane of
+// `warp` calls it): one reservation per warp, the slots written (waiting, bounded, for a slot the
+// ring's previous lap has not yet read), then one fence and the count published in free_avail.
+// ring_cap >= capacity + kMaxSmSlots * chunk: the entries written and not yet read (free nodes,
+// and the rest of per-SM chunks taken from the ring) never fill the ring, so a pusher meets a
+// slot of the previous lap only while its reader is about to clear it.
+template <class Warp>
+MVBT_DEV void ring_push(control_block* c, bool freed, uint32_t node, const Warp& warp) {
+  const uint32_t m = warp.ballot(freed);
+  if (!m) return;
+  const uint32_t lane = warp.thread_rank();
+  const int lead      = __ffs(m) - 1;
+  unsigned long long base = 0;
+  if ((int)lane == lead) base = atomicAdd(&c->free_tail, (unsigned long long)__popc(m));
+  base = warp.shfl(base, lead);
+  if (freed) {
+    uint32_t* slot = reinterpret_cast<uint32_t*>(c->free_ring) +
+                     ((base + __popc(m & ((1u << lane) - 1u))) & (c->ring_cap - 1u));
+    const unsigned long long t0 = global_ns();
+    while (ld_relaxed_u32(slot) != kRingEmpty && global_ns() - t0 <= c->wait_ns) __nanosleep(64);
+    st_relaxed_u32(slot, node);
+  }
+  __threadfence();
+  warp.sync();
+  if ((int)lane == lead) {
+    atomicAdd(&c->free_avail, (unsigned long long)__popc(m));
+    atomicAdd(&c->stat_reclaimed, (unsigned long long)__popc(m));
+  }
 }
 // Records a version copy in the retire log. A copy the full log cannot take is never freed
 // (counted in stat_log_dropped).
@@ -776,11 +839,13 @@ struct device_tree {
   template <class Tile>
   MVBT_DEV uint32_t alloc(const Tile& t) const {
     uint32_t idx = kNone;
-    if (t.thread_rank() == 0) idx = alloc_one();
-    idx = t.shfl(idx, 0);
-    // a position in the free ring (a chunk of reclaimed nodes): the node stored there
-    if (idx != kNone && (idx & kRingChunk)) idx = chunk_node(ctl, idx, 0);
-    return idx;
+    if (t.thread_rank() == 0) {
+      idx = alloc_one();
+      // a position in the free ring (a chunk of reclaimed nodes): the node stored there, read
+      // once (reading clears the slot), by this lane alone
+      if (idx != kNone && (idx & kRingChunk)) idx = chunk_node(ctl, idx, 0);
+    }
+    return t.shfl(idx, 0);
   }
 
   // ---- locks on the mod word ----
@@ -810,7 +875,7 @@ struct device_tree {
         if (!(cur & kLockBit)) break;
         backoff = backoff < 1024 ? backoff * 2 : 1024;
       }
-      if (global_ns() - t0 > lns) break;
+      if (wait_expired(t0, lns, t)) break;
     }
     if (t.thread_rank() == 0) set_error(kErrSpinLimit, 2);
     return false;
@@ -869,68 +934,65 @@ struct device_tree {
     else
       atomicAdd(&ctl->sm_stats[sm_id() % kMaxSmSlots][0], 1ull);
   }
-  // One entry of a reclaim pass over the retire log; no writer runs during a pass. A copy made in
-  // epoch E is read only at snapshots below E, so with no live snapshot below the watermark M it
-  // is unreachable once E <= M (compared in a window of 2^28 epochs). Returns 1 if the entry's
-  // copy is now marked free (the caller appends idx to the free ring), 2 if it must be kept, 0 if
-  // the entry was consumed by an earlier pass.
-  MVBT_DEV int reclaim_entry(unsigned long long pos, uint32_t M, uint32_t& idx) const {
+  // One retire-log entry at position pos. A copy made in epoch E is read only at snapshots below
+  // E, so with no live snapshot below the watermark M it is unreachable once E <= M (compared in a
+  // window of 2^28 epochs). Returns 1 if the entry's copy is now marked free (the caller appends
+  // idx to the free ring), 2 if it must be kept, 0 if the entry holds nothing (consumed, or a copy
+  // the full log dropped). A consumed or freed entry's slot is cleared. check_epoch = false: the
+  // caller knows the position holds a reclaimable copy (reclaim_online).
+  MVBT_DEV int reclaim_entry(unsigned long long pos, uint32_t M, uint32_t& idx, bool check_epoch = true) const {
     control_block* c = ctl;
     uint32_t* slot   = reinterpret_cast<uint32_t*>(c->retire_log) + (pos & (c->reclaim_cap - 1u));
-    idx              = *slot;
+    idx              = ld_relaxed_u32(slot);
     if (idx >= capacity) return 0;
     uint32_t* mod    = node_ptr(idx) + kModWord;
-    const uint32_t m = *mod;
+    const uint32_t m = ld_relaxed_u32(mod);
     if (!(m & kRetiredBit)) {
-      *slot = kNone;
+      st_relaxed_u32(slot, kNone);
       return 0;
     }
-    if (((M - m) & kCountMask) > (kCountMask >> 1)) return 2;  // made after the watermark
-    *mod  = kFreeBit;
-    *slot = kNone;
+    if (check_epoch && ((M - m) & kCountMask) > (kCountMask >> 1)) return 2;  // made after the watermark
+    st_relaxed_u32(mod, kFreeBit);
+    st_relaxed_u32(slot, kNone);
     return 1;
   }
-  // End of a reclaim pass, per-SM slot s: the unused rest of its chunk goes back to the free ring
-  // (at positions from ring_tail + *pending on) and the slot is emptied, so no chunk refers to ring
-  // positions a later pass may write. Returns the number of nodes handed back.
-  template <class AddPending>
-  MVBT_DEV uint32_t reclaim_return_chunk(int s, unsigned long long ring_tail, AddPending add_pending) const {
-    control_block* c              = ctl;
-    const uint32_t C              = c->chunk;
-    const unsigned long long v    = c->sm_pool[s];
-    const uint32_t base = (uint32_t)(v >> 32), used = (uint32_t)v;
-    uint32_t n = 0;
-    if (used < C) {
-      n                = C - used;
-      const uint32_t k = add_pending(n);
-      uint32_t* ring   = reinterpret_cast<uint32_t*>(c->free_ring);
-      for (uint32_t u = 0; u < n; ++u) ring[(ring_tail + k + u) & (c->ring_cap - 1u)] = chunk_node(c, base, used + u);
-    }
-    c->sm_pool[s] = C;  // empty: the next allocation on this SM refills
-    return n;
-  }
-  // End of a reclaim pass (one thread, after every entry and every chunk): publishes the
-  // `pushed` ring entries, counts the `freed` copies, moves the log head past consumed entries.
-  // retire_tail stays the count of every copy made. Positions beyond head + capacity were never
-  // written (those copies were dropped); they alias slots this pass marked consumed, so a later
-  // pass passes over them.
-  MVBT_DEV void reclaim_publish(uint32_t pushed, uint32_t freed) const {
+  // End of a reclaim pass between kernels (one thread, after every entry): moves the log head
+  // past the consumed entries, up to the first copy the pass had to keep. retire_tail stays the
+  // count of every copy made. Positions beyond head + capacity were never written (those copies
+  // were dropped); they alias slots this pass cleared, so a later pass passes over them.
+  MVBT_DEV void reclaim_publish() const {
     control_block* c              = ctl;
     const unsigned long long head = c->retire_head;
     unsigned long long n          = c->retire_tail - head;
     if (n > c->reclaim_cap) n = c->reclaim_cap;
     const uint32_t keep = c->rc_first_kept;
     c->retire_head      = head + (keep == 0xFFFFFFFFu ? n : keep);
-    unsigned long long fh = c->free_head;
-    if (c->ring_fail < fh) fh = c->ring_fail;  // failed pops handed nothing out
-    c->stat_reused += fh - c->free_mark;
-    c->free_head = fh;
-    c->free_mark = fh;
-    c->ring_fail = ~0ull;
-    c->free_tail += pushed;
-    c->stat_reclaimed += freed;
-    c->rc_pending    = 0;
-    c->rc_first_kept = 0xFFFFFFFFu;
+    c->rc_first_kept    = 0xFFFFFFFFu;
+  }
+  // Reclamation while kernels run (warp-collective): claims up to 32 retire-log positions below
+  // `limit` -- positions the caller knows hold only copies that no live snapshot reads -- frees
+  // their copies and appends them to the free ring. Returns the number of positions claimed.
+  template <class Warp>
+  MVBT_DEV uint32_t reclaim_online(unsigned long long limit, const Warp& warp) const {
+    control_block* c       = ctl;
+    unsigned long long h   = 0;
+    uint32_t n             = 0;
+    if (warp.thread_rank() == 0) {
+      h = ld_relaxed_u64(&c->retire_head);
+      if (h < limit) {
+        n = (uint32_t)(limit - h < 32 ? limit - h : 32);
+        if (atomicCAS(&c->retire_head, h, h + n) != h) n = 0;  // another warp took them
+      }
+    }
+    h = warp.shfl(h, 0);
+    n = warp.shfl(n, 0);
+    if (n == 0) return 0;
+    __threadfence();  // the copies' last readers finished before `limit` was published
+    const uint32_t lane = warp.thread_rank();
+    uint32_t idx        = kNone;
+    const bool freed    = lane < n && reclaim_entry(h + lane, 0, idx, false) == 1;
+    ring_push(c, freed, idx, warp);
+    return n;
   }
 
   // Moves from node idx to the version visible at ts (snapshot readers only). Sets `copy` when it
@@ -981,7 +1043,7 @@ struct device_tree {
       const uint32_t mod1 = ld_relaxed_u32(p + kModWord);
       const bool torn     = (mod0 & kLockBit) != 0 || mod0 != mod1;
       if (t.ballot(torn) == 0) return true;
-      if (global_ns() - t0 > lim) break;
+      if (wait_expired(t0, lim, t)) break;
       __nanosleep(backoff);
       backoff = backoff < 1024 ? backoff * 2 : 1024;
     }
@@ -1677,7 +1739,19 @@ struct batch_sched {
   uint32_t* done_batches;        // zero at launch
   unsigned long long* wcursor;   // next write ordinal (zero at launch)
   unsigned long long* rcursor;   // next read ordinal (zero at launch)
-  const uint32_t* params;        // [0] num_batches, [1] snapshot of batch 0
+  const uint32_t* params;        // [0] num_batches, [1] snapshot of batch 0, [2] external watermark
+  // Reclamation inside the launch (all null: off). A copy made in epoch E is read only at
+  // snapshots below E; batch b writes in epoch S0 + b + 1 and reads at S0 + b. So once batches
+  // 0..b have finished their writes and their reads, the copies batch b and earlier made (all at
+  // retire-log positions below the log tail read when batch b's writes had finished) are read by
+  // no snapshot of this launch; params[2] is the caller's watermark: the oldest snapshot it still
+  // reads outside the launch (copies made in later epochs are kept; kReclaimAll: none held).
+  uint32_t* reads_done            = nullptr;  // [nb] finished reads (zero at launch)
+  uint32_t* full_done             = nullptr;  // leading batches with writes and reads all finished
+  unsigned long long* tail_at     = nullptr;  // [nb] log tail once batch b's writes finished (~0: not yet)
+  unsigned long long* rc_limit    = nullptr;  // log positions below it are reclaimable
+  unsigned long long* series      = nullptr;  // [nb][4] when batch b's writes finished: epoch, bump,
+                                              // free_avail, stat_reclaimed (memory over time)
 };
 
 constexpr uint32_t kWriteClaim = 1;  // writes per tile per claim
@@ -1697,14 +1771,50 @@ MVBT_DEV uint32_t batch_of_ordinal(const uint64_t* pre, uint32_t nb, uint64_t x,
   return lo;
 }
 
-// Advances done_batches past every leading batch whose writes are all finished (lane 0 only).
-MVBT_DEV void advance_done(const batch_sched& sc, uint32_t nb) {
+// Advances done_batches past every leading batch whose writes are all finished (lane 0 only). With
+// reclamation on, the thread that advances past batch d records the retire-log tail (read after
+// d's writes finished and before any write of d + 1 can start) and a memory sample.
+MVBT_DEV void advance_done(const batch_sched& sc, uint32_t nb, control_block* ctl = nullptr) {
   uint32_t d = ld_relaxed_u32(sc.done_batches);
   while (d < nb) {
     if (ld_relaxed_u32(&sc.writes_done[d]) < sc.n_writes[d]) break;
     __threadfence();
+    const unsigned long long tail = (sc.tail_at && ctl) ? ld_relaxed_u64(&ctl->retire_tail) : 0ull;
     uint32_t prev = atomicCAS(sc.done_batches, d, d + 1);
+    if (prev == d && sc.tail_at && ctl) {
+      if (sc.series) {
+        unsigned long long* e = sc.series + 4ull * d;
+        e[0] = ld_relaxed_u32(sc.params + 1) + d + 1u;
+        e[1] = ld_relaxed_u32(&ctl->bump);
+        e[2] = ld_relaxed_u64(&ctl->free_avail);
+        e[3] = ld_relaxed_u64(&ctl->stat_reclaimed);
+      }
+      atomicExch(&sc.tail_at[d], tail);
+    }
     d = (prev == d) ? d + 1 : prev;
+  }
+}
+
+// Reclamation on: advances full_done past every leading batch whose writes and reads are all
+// finished and raises rc_limit to the log tail recorded for it (lane 0 only).
+MVBT_DEV void advance_full(const batch_sched& sc, uint32_t nb) {
+  uint32_t f       = ld_relaxed_u32(sc.full_done);
+  const uint32_t d = ld_relaxed_u32(sc.done_batches);
+  const uint32_t S0 = ld_relaxed_u32(sc.params + 1), ext = ld_relaxed_u32(sc.params + 2);
+  while (f < d && f < nb) {
+    const uint32_t reads = (uint32_t)(sc.batch_off[f + 1] - sc.batch_off[f]) - sc.n_writes[f];
+    if (ld_relaxed_u32(&sc.reads_done[f]) < reads) break;
+    __threadfence();
+    const unsigned long long t = ld_relaxed_u64(&sc.tail_at[f]);
+    if (t == ~0ull) break;  // its writes' advancer has not recorded the tail yet
+    const uint32_t prev = atomicCAS(sc.full_done, f, f + 1);
+    if (prev == f) {
+      // batch f's copies were made in epoch S0 + f + 1: free only at or below the watermark
+      if (ext == kReclaimAll || S0 + f + 1u <= ext) atomicMax(sc.rc_limit, t);
+      ++f;
+    } else {
+      f = prev;
+    }
   }
 }
 
@@ -1716,7 +1826,7 @@ MVBT_DEV bool wait_batch_ready(const device_tree& T, const batch_sched& sc, uint
   for (uint32_t w = 0;; ++w) {
     uint32_t d = 0;
     if (t.thread_rank() == 0) {
-      advance_done(sc, nb);
+      advance_done(sc, nb, T.ctl);
       d = ld_relaxed_u32(sc.done_batches);
     }
     d = t.shfl(d, 0);
@@ -1725,8 +1835,37 @@ MVBT_DEV bool wait_batch_ready(const device_tree& T, const batch_sched& sc, uint
       t.sync();
       return true;
     }
-    if (global_ns() - t0 > T.ctl->wait_ns) return false;
+    if (wait_expired(t0, T.ctl->wait_ns, t)) return false;
     __nanosleep(w < 8 ? 128 : 1024);
+  }
+}
+
+// One step of reclamation inside the launch (warp-collective): advances full_done, then frees up
+// to 32 copies below rc_limit. Returns true if it claimed any log position.
+template <class Warp>
+MVBT_DEV bool reclaim_step(const device_tree& T, const batch_sched& sc, uint32_t nb, const Warp& warp) {
+  unsigned long long lim = 0;
+  if (warp.thread_rank() == 0) {
+    advance_full(sc, nb);
+    lim = ld_relaxed_u64(sc.rc_limit);
+  }
+  lim = warp.shfl(lim, 0);
+  return T.reclaim_online(lim, warp) > 0;
+}
+// At the end of a warp's work: reclaim while there is reclaimable work, bounded by the wait limit
+// (the last batches' reads may still be running in other warps; what is left waits for the next
+// launch or a pass between launches).
+template <class Warp>
+MVBT_DEV void reclaim_drain(const device_tree& T, const batch_sched& sc, uint32_t nb, const Warp& warp) {
+  const unsigned long long t0 = global_ns();
+  for (uint32_t idle = 0; idle < 4 && !wait_expired(t0, T.ctl->wait_ns, warp);) {
+    if (warp.thread_rank() == 0) advance_done(sc, nb, T.ctl);
+    if (reclaim_step(T, sc, nb, warp)) {
+      idle = 0;
+    } else {
+      ++idle;
+      __nanosleep(512);
+    }
   }
 }
 
@@ -1756,7 +1895,11 @@ MVBT_DEV void batched_worker(const device_tree& T, const batch_view& B, const ba
     d = warp.shfl(d, 0);
     g = warp.shfl(g, 0);
     r = warp.shfl(r, 0);
-    if (g >= TW && r >= TR) break;
+    if (g >= TW && r >= TR) {
+      // all work is claimed: help reclaim what the finished batches no longer need, then leave
+      if (sc.rc_limit) reclaim_drain(T, sc, nb, warp);
+      break;
+    }
     __threadfence();  // the batches counted in d are finished: see their writes
     warp.sync();
     bool did = false;
@@ -1801,7 +1944,9 @@ MVBT_DEV void batched_worker(const device_tree& T, const batch_view& B, const ba
         r0 = warp.shfl(r0, 0);
         did = r0 < TR;
         uint32_t b = rb, dd = d;
+        uint32_t done_b[kReadClaim];  // batch of each read this tile ran (counted after a fence)
         for (uint32_t k = 0; k < kReadClaim; ++k) {
+          done_b[k]                  = 0xFFFFFFFFu;
           const unsigned long long x = r0 + k * kTiles + tid;
           if (x >= TR) break;
           b = batch_of_ordinal(sc.rpre, nb, x, b);
@@ -1815,6 +1960,14 @@ MVBT_DEV void batched_worker(const device_tree& T, const batch_view& B, const ba
           } else {
             run_batch_op<W>(T, B, i, S0 + b, S0 + b + 1, t);
           }
+          done_b[k] = b;
+        }
+        if (sc.reads_done) {  // the reads' loads are complete before they are counted
+          __threadfence();
+          t.sync();
+          if (t.thread_rank() == 0)
+            for (uint32_t k = 0; k < kReadClaim; ++k)
+              if (done_b[k] != 0xFFFFFFFFu) atomicAdd(&sc.reads_done[done_b[k]], 1u);
         }
       }
     }
@@ -1823,10 +1976,15 @@ MVBT_DEV void batched_worker(const device_tree& T, const batch_view& B, const ba
       idle_since = 0;
       continue;
     }
-    // nothing runnable yet: help advance done_batches, then back off (bounded)
-    if (warp.thread_rank() == 0) advance_done(sc, nb);
+    // nothing runnable yet: help advance done_batches, reclaim, then back off (bounded)
+    if (warp.thread_rank() == 0) advance_done(sc, nb, T.ctl);
+    if (sc.rc_limit && reclaim_step(T, sc, nb, warp)) {
+      spin       = 0;
+      idle_since = 0;
+      continue;
+    }
     if (idle_since == 0) idle_since = global_ns();
-    if (global_ns() - idle_since > T.ctl->wait_ns) {
+    if (wait_expired(idle_since, T.ctl->wait_ns, warp)) {
       if (warp.thread_rank() == 0) T.set_error(kErrSpinLimit, 14);
       break;
     }

@@ -61,12 +61,14 @@ class mvbt_serve_config(ctypes.Structure):
     _fields_ = [("max_ops_per_launch", _u64), ("max_range_pairs", _u64),
                 ("max_requests_per_launch", _u32), ("pipeline_depth", _u32), ("mode", _u32),
                 ("reclaim_every", _u32), ("nodes_per_write", _u32), ("snapshots", _u32),
-                ("reserve_nodes", _u64), ("reserved", _u64 * 4)]
+                ("reserve_nodes", _u64), ("reclaim_in_launch", _u32), ("pad0", _u32),
+                ("max_reclaim_lag", _u64), ("reserved", _u64 * 2)]
 
 
 class mvbt_serve_stats(ctypes.Structure):
     _fields_ = [(n, _u64) for n in ("requests", "ops", "launches", "reclaims", "span_ns", "max_waiting",
-                                     "memory_waits", "max_launch_ops")] + [("reserved", _u64 * 8)]
+                                     "memory_waits", "max_launch_ops", "max_reclaim_lag", "lag_waits",
+                                     "nodes_high_water")] + [("reserved", _u64 * 5)]
 
 
 def _sig(name, res, *args):
@@ -104,6 +106,8 @@ _sig("mvbt_batch_plan_create", ctypes.c_int, _vp, _u64, _u32, ctypes.POINTER(_vp
 _sig("mvbt_batch_plan_destroy", ctypes.c_int, _vp)
 _sig("mvbt_batch_run", ctypes.c_int, _vp, _u32, _vp, _P, _P, _P, _P, _P, _P, _P, ctypes.c_int, _vp)
 _sig("mvbt_batch_plan_timing", ctypes.c_int, _vp, ctypes.c_int)
+_sig("mvbt_batch_plan_set_reclaim", ctypes.c_int, _vp, ctypes.c_int, _u32)
+_sig("mvbt_batch_plan_memory_series", ctypes.c_int, _vp, _vp, _u32, ctypes.POINTER(_u32))
 _sig("mvbt_batch_plan_kernel_times", ctypes.c_int, _vp, ctypes.POINTER(ctypes.c_float), _u32,
      ctypes.POINTER(_u32))
 _sig("mvbt_stats", ctypes.c_int, _vp, ctypes.POINTER(_u64), _u32)
@@ -505,6 +509,7 @@ class BatchPlan:
                "batch_plan_create")
         self._h = h
         self.tree = tree  # keeps the tree alive while the plan exists
+        self.max_batches = int(max_batches)
 
     def run(self, batch_off, type, key, arg, out_off, range_cap, result, range_out,
             mode: int = BATCH_PERSISTENT, stream=None):
@@ -533,6 +538,22 @@ class BatchPlan:
         blocks per SM (-1 = the tree's, 0 = full occupancy, 4 / 6 / 8 = register-capped variants)."""
         _check(lib.mvbt_batch_plan_set_launch(self._h, int(tile_width), int(blocks_per_sm)), "set_launch")
         self.launch = (int(tile_width), int(blocks_per_sm))
+
+    def set_reclaim(self, enable: bool = True, min_live_snapshot: int = 0xFFFFFFFF) -> None:
+        """Reclamation inside this plan's persistent runs (the tree needs reclaim=True):
+        min_live_snapshot is the oldest snapshot still read outside the runs (RECLAIM_ALL: none)."""
+        _check(lib.mvbt_batch_plan_set_reclaim(self._h, int(bool(enable)), int(min_live_snapshot)), "set_reclaim")
+
+    def memory_series(self):
+        """Per batch of the last persistent run with reclamation on, sampled when its writes had
+        finished: uint64 array [batches, 4] = epoch, nodes taken from the pool, freed nodes waiting
+        in the free ring, nodes freed so far (live nodes = column 1 - column 2)."""
+        import numpy as np
+        out = np.zeros((self.max_batches, 4), np.uint64)
+        n = _u32(0)
+        _check(lib.mvbt_batch_plan_memory_series(self._h, out.ctypes.data, self.max_batches, ctypes.byref(n)),
+               "memory_series")
+        return out[: n.value]
 
     def enable_timing(self, on: bool = True) -> None:
         """CUDA events around the persistent kernel of each BATCH_PERSISTENT run."""

@@ -60,9 +60,18 @@ struct mvbt_batch_plan {
   // end of the plan's last persistent / graph run: its pinned staging is free once it completes
   cudaEvent_t staging_ev = nullptr;
   bool staging_pending   = false;
+  // reclamation inside the persistent runs (mvbt_batch_plan_set_reclaim): reads_done[mb] |
+  // full_done, padded to 8-byte words (rc_head_words) | tail_at[mb] | rc_limit | series[4 * mb]
+  bool reclaim_on              = false;
+  uint32_t reclaim_watermark   = 0xFFFFFFFFu;
+  void* d_rc                   = nullptr;
+  uint32_t series_batches      = 0;  // batches of the last persistent run with reclamation on
 };
 
 namespace {
+
+// uint32 words of the reclamation scratch before its 64-bit part (reads_done[mb], full_done, pad)
+inline uint64_t rc_head_words(uint64_t mb) { return (mb + 2) & ~1ull; }
 
 constexpr int kPrepassBlocks = 512;
 constexpr int kPrepassThreads = 256;
@@ -189,6 +198,18 @@ __global__ void k_batch_begin(mvbt::control_block* ctl, uint32_t* params) {
   }
 }
 
+// Reclamation on: the copies made before this launch (epochs <= its first snapshot S0) are read
+// by no snapshot of the launch, so they are reclaimable from the start unless the caller still
+// reads a snapshot below S0 (watermark params[2] < S0).
+__global__ void k_batch_begin_reclaim(mvbt::control_block* ctl, const uint32_t* params,
+                                      unsigned long long* rc_limit) {
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const uint32_t S0 = params[1], ext = params[2];
+    *rc_limit = (ext == mvbt::kReclaimAll || S0 <= ext) ? ctl->retire_tail : ctl->retire_head;
+  }
+}
+
 __global__ void k_batch_end(mvbt::control_block* ctl, const uint32_t* params) {
   if (threadIdx.x == 0) {
     __threadfence();
@@ -253,8 +274,19 @@ int enqueue_persistent(mvbt_batch_plan* p, const launch_ctx& c, const batch_view
   const uint32_t mb = p->max_batches;
   MVBT_TRY(cudaMemcpyAsync(p->d_batch_off, p->h_batch_off, (mb + 1) * sizeof(uint64_t),
                            cudaMemcpyHostToDevice, s));
-  MVBT_TRY(cudaMemcpyAsync(p->d_params, p->h_params, 2 * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+  MVBT_TRY(cudaMemcpyAsync(p->d_params, p->h_params, 3 * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
   MVBT_TRY(cudaMemsetAsync(p->d_counts, 0, (6ull * mb + 4) * sizeof(uint32_t), s));
+  uint32_t* rc_reads            = nullptr;
+  unsigned long long* rc_tail   = nullptr;
+  unsigned long long* rc_series = nullptr;
+  if (p->reclaim_on) {
+    rc_reads  = static_cast<uint32_t*>(p->d_rc);
+    rc_tail   = reinterpret_cast<unsigned long long*>(rc_reads + rc_head_words(mb));
+    rc_series = rc_tail + mb + 1;
+    MVBT_TRY(cudaMemsetAsync(rc_reads, 0, rc_head_words(mb) * sizeof(uint32_t), s));
+    MVBT_TRY(cudaMemsetAsync(rc_tail, 0xFF, mb * sizeof(unsigned long long), s));
+    MVBT_TRY(cudaMemsetAsync(rc_series, 0, 4ull * mb * sizeof(unsigned long long), s));
+  }
   MVBT_TRY(cudaMemsetAsync(p->d_cursor, 0, 2 * sizeof(unsigned long long), s));
   uint32_t* nw    = p->d_counts;
   uint32_t* nf    = p->d_counts + mb;
@@ -268,6 +300,7 @@ int enqueue_persistent(mvbt_batch_plan* p, const launch_ctx& c, const batch_view
                                                      mb, p->d_perm);
   k_prefix<<<1, 1024, 0, s>>>(p->d_batch_off, p->d_params, nw, wpre, rpre);
   k_batch_begin<<<1, 32, 0, s>>>(c.ctl, p->d_params);
+  if (p->reclaim_on) k_batch_begin_reclaim<<<1, 32, 0, s>>>(c.ctl, p->d_params, rc_tail + mb);
   batch_sched sc;
   sc.batch_off    = p->d_batch_off;
   sc.perm         = p->d_perm;
@@ -279,6 +312,13 @@ int enqueue_persistent(mvbt_batch_plan* p, const launch_ctx& c, const batch_view
   sc.wcursor      = p->d_cursor;
   sc.rcursor      = p->d_cursor + 1;
   sc.params       = p->d_params;
+  if (p->reclaim_on) {
+    sc.reads_done = rc_reads;
+    sc.full_done  = rc_reads + mb;
+    sc.tail_at    = rc_tail;
+    sc.rc_limit   = rc_tail + mb;
+    sc.series     = rc_series;
+  }
   const int slot = (int)(p->timed_runs % mvbt_batch_plan::kTimed);
   if (p->timing) cudaEventRecord(p->ev_begin[slot], s);
   if (c.W == 8) launch_batched<8>(c, B, sc, s);
@@ -355,6 +395,7 @@ int mvbt_batch_plan_destroy(mvbt_batch_plan* p) {
   cudaFreeHost(p->h_batch_off);
   cudaFreeHost(p->h_params);
   if (p->d_scratch) cudaFree(p->d_scratch);
+  if (p->d_rc) cudaFree(p->d_rc);
   if (p->staging_ev) cudaEventDestroy(p->staging_ev);
   mvbt_batch_plan_timing(p, 0);
   delete p;
@@ -405,6 +446,8 @@ int mvbt_internal_batch_enqueue(mvbt_batch_plan* p, uint32_t num_batches, const 
   for (uint32_t b = num_batches + 1; b <= p->max_batches; ++b) p->h_batch_off[b] = total;
   p->h_params[0] = num_batches;
   p->h_params[1] = 0;
+  p->h_params[2] = p->reclaim_watermark;
+  if (p->reclaim_on) p->series_batches = num_batches;
   batch_view B;
   B.type      = type;
   B.key       = key;
@@ -474,6 +517,8 @@ int mvbt_batch_run(mvbt_batch_plan* p, uint32_t num_batches, const uint64_t* bat
   for (uint32_t b = num_batches + 1; b <= p->max_batches; ++b) p->h_batch_off[b] = total;
   p->h_params[0] = num_batches;
   p->h_params[1] = 0;
+  p->h_params[2] = p->reclaim_watermark;
+  if (p->reclaim_on) p->series_batches = num_batches;
 
   if (!p->staging_ev) MVBT_TRY(cudaEventCreateWithFlags(&p->staging_ev, cudaEventDisableTiming));
   if (mode == MVBT_BATCH_PERSISTENT) {
@@ -511,6 +556,46 @@ int mvbt_batch_run(mvbt_batch_plan* p, uint32_t num_batches, const uint64_t* bat
   MVBT_TRY(cudaGraphLaunch(p->graph, s));
   MVBT_TRY(cudaEventRecord(p->staging_ev, s));
   p->staging_pending = true;
+  return MVBT_OK;
+}
+
+int mvbt_batch_plan_set_reclaim(mvbt_batch_plan* p, int enable, uint32_t min_live_snapshot) {
+  if (!p) return fail(MVBT_ERR_BAD_ARG, "null plan");
+  device_tree v;
+  int W, bs, sms;
+  uint32_t bps, maxb;
+  void* ctl;
+  int st = mvbt_internal_view(p->tree, &v, &W, &bs, &sms, &bps, &maxb, &ctl);
+  if (st) return st;
+  if (enable && !v.reclaim)
+    return fail(MVBT_ERR_NOT_SUPPORTED, "reclamation is off: create the tree with mvbt_config.reclaim = 1");
+  if (enable && !p->d_rc) {
+    const uint64_t mb    = p->max_batches;
+    const uint64_t bytes = rc_head_words(mb) * 4 + (mb + 1) * 8 + 4 * mb * 8;
+    if (cudaMalloc(&p->d_rc, bytes) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(MVBT_ERR_OUT_OF_MEMORY, "batch plan: reclamation scratch");
+    }
+  }
+  if (p->have_graph && p->reclaim_on != (enable != 0)) {  // the captured run changes shape
+    cudaGraphExecDestroy(p->graph);
+    p->have_graph = false;
+  }
+  p->reclaim_on        = enable != 0;
+  p->reclaim_watermark = min_live_snapshot;
+  return MVBT_OK;
+}
+
+int mvbt_batch_plan_memory_series(mvbt_batch_plan* p, uint64_t* out, uint32_t max_batches, uint32_t* n) {
+  if (!p || !out || !n) return fail(MVBT_ERR_BAD_ARG, "null argument");
+  *n = 0;
+  if (!p->d_rc || p->series_batches == 0) return MVBT_OK;
+  if (p->staging_pending) MVBT_TRY(cudaEventSynchronize(p->staging_ev));
+  const uint32_t k = std::min(max_batches, p->series_batches);
+  const uint64_t mb = p->max_batches;
+  auto* series = reinterpret_cast<unsigned long long*>(static_cast<uint32_t*>(p->d_rc) + rc_head_words(mb)) + mb + 1;
+  MVBT_TRY(cudaMemcpy(out, series, 4ull * k * sizeof(uint64_t), cudaMemcpyDeviceToHost));
+  *n = k;
   return MVBT_OK;
 }
 

@@ -48,13 +48,15 @@ int fail(int code, const std::string& msg) {
   return code;
 }
 
-// Node usage after a launch: [0] bump pointer, [1] reclaimed nodes waiting for reuse, [2] epoch.
+// Node usage after a launch: [0] bump pointer, [1] reclaimed nodes waiting for reuse, [2] epoch,
+// [3] reclamation lag: version copies retired and not yet freed (retire-log entries).
 __global__ void k_usage(const mvbt::control_block* c, unsigned long long* out) {
   if (threadIdx.x == 0) {
-    const unsigned long long fh = c->ring_fail < c->free_head ? c->ring_fail : c->free_head;
+    const long long avail = (long long)c->free_avail;
     out[0] = c->bump;
-    out[1] = c->reclaim_cap ? c->free_tail - fh : 0ull;
+    out[1] = c->reclaim_cap && avail > 0 ? (unsigned long long)avail : 0ull;
     out[2] = c->epoch;
+    out[3] = c->reclaim_cap ? c->retire_tail - c->retire_head : 0ull;
   }
 }
 
@@ -157,8 +159,8 @@ int mvbt_serve_trace(mvbt_tree* tree, const mvbt_serve_config* cfg_in, uint32_t 
   void* ctl = nullptr;
   st = mvbt_internal_view(tree, &view, &W, &block, &sms, &bps, &maxb, &ctl);
   if (st) return st;
-  if (cfg.reclaim_every && !view.reclaim)
-    return fail(MVBT_ERR_NOT_SUPPORTED, "reclaim_every needs a tree created with config.reclaim = 1");
+  if ((cfg.reclaim_every || cfg.reclaim_in_launch || cfg.max_reclaim_lag) && !view.reclaim)
+    return fail(MVBT_ERR_NOT_SUPPORTED, "reclamation needs a tree created with config.reclaim = 1");
   const uint32_t max_req = cfg.mode == MVBT_BATCH_PER_LAUNCH ? 1u : cfg.max_requests_per_launch;
   // batches per launch: one per request, or the whole admitted group as one batch
   const bool per_request = cfg.snapshots == MVBT_SERVE_SNAPSHOT_PER_REQUEST;
@@ -201,6 +203,11 @@ int mvbt_serve_trace(mvbt_tree* tree, const mvbt_serve_config* cfg_in, uint32_t 
   for (auto& s : S.slots) {
     st = mvbt_batch_plan_create(tree, mo, per_request ? max_req : 1u, &s.plan);
     if (st) return st;
+    // every snapshot of the session is taken and read inside its launch: none is held outside
+    if (cfg.reclaim_in_launch && cfg.mode == MVBT_BATCH_PERSISTENT) {
+      st = mvbt_batch_plan_set_reclaim(s.plan, 1, MVBT_RECLAIM_ALL);
+      if (st) return st;
+    }
     SERVE_TRY(cudaMalloc(&s.type, mo * 4));
     SERVE_TRY(cudaMalloc(&s.key, mo * 4));
     SERVE_TRY(cudaMalloc(&s.arg, mo * 4));
@@ -221,6 +228,8 @@ int mvbt_serve_trace(mvbt_tree* tree, const mvbt_serve_config* cfg_in, uint32_t 
   const uint64_t capacity = view.capacity;
   uint64_t in_use         = S.slots[0].usage[0] - S.slots[0].usage[1];
   uint32_t epoch          = (uint32_t)S.slots[0].usage[2];
+  uint64_t lag            = S.slots[0].usage[3];
+  uint64_t max_lag = lag, lag_waits = 0, high_water = in_use;
 
   using clk      = std::chrono::steady_clock;
   const auto t0  = clk::now();
@@ -312,7 +321,10 @@ int mvbt_serve_trace(mvbt_tree* tree, const mvbt_serve_config* cfg_in, uint32_t 
       for (uint32_t r = s.r0; r < s.r1; ++r) done_ns[r] = t;
       ndone += s.r1 - s.r0;
       reserved -= s.reserve;
-      in_use = s.usage[0] - s.usage[1];
+      in_use     = s.usage[0] - s.usage[1];
+      lag        = s.usage[3];
+      max_lag    = std::max(max_lag, lag);
+      high_water = std::max(high_water, in_use);
       s.busy = false;
       inflight.pop_front();
       progress = true;
@@ -320,8 +332,27 @@ int mvbt_serve_trace(mvbt_tree* tree, const mvbt_serve_config* cfg_in, uint32_t 
     const uint64_t tnow = now_ns();
     while (arrived < R && arrival[arrived] <= tnow) ++arrived;
     max_waiting = std::max<uint64_t>(max_waiting, arrived - next);
+    // admission by reclamation lag: too many copies wait in the retire log -- reclaim first
+    if (cfg.max_reclaim_lag && lag > cfg.max_reclaim_lag && next < arrived && inflight.size() < S.slots.size()) {
+      ++lag_waits;
+      if (inflight.empty()) {
+        int rs = mvbt_reclaim(tree, MVBT_RECLAIM_ALL, S.cs);
+        if (rs) return rs;
+        ++reclaims;
+        since_reclaim = 0;
+        k_usage<<<1, 32, 0, S.cs>>>(cb, S.slots[0].usage_dev);
+        SERVE_TRY(cudaStreamSynchronize(S.cs));
+        in_use        = S.slots[0].usage[0] - S.slots[0].usage[1];
+        lag           = S.slots[0].usage[3];
+        force_reclaim = false;
+        progress      = true;
+      } else {
+        force_reclaim = true;  // the next launch starts with a pass
+      }
+    }
     // admission into a free slot
-    if (next < arrived && inflight.size() < S.slots.size()) {
+    if (next < arrived && inflight.size() < S.slots.size() &&
+        !(cfg.max_reclaim_lag && lag > cfg.max_reclaim_lag && force_reclaim)) {
       int si = 0;
       while (S.slots[si].busy) ++si;
       const uint64_t gstart = rp0[next];
@@ -389,6 +420,9 @@ int mvbt_serve_trace(mvbt_tree* tree, const mvbt_serve_config* cfg_in, uint32_t 
     stats->max_waiting    = max_waiting;
     stats->memory_waits   = mem_waits;
     stats->max_launch_ops = max_launch_ops;
+    stats->max_reclaim_lag  = max_lag;
+    stats->lag_waits        = lag_waits;
+    stats->nodes_high_water = high_water;
   }
   return MVBT_OK;
 }

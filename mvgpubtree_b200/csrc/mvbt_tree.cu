@@ -89,15 +89,14 @@ __global__ void k_init(uint32_t* pool, control_block* c, uint32_t capacity, uint
 }
 
 // Reclaim pass over the retire log (mvbt_reclaim): frees every version copy made in an epoch <= M
-// (kReclaimAll: the current epoch). Warp-aggregated appends to the free ring.
+// (kReclaimAll: the current epoch) and appends it to the free ring (one reservation per warp).
 __global__ void __launch_bounds__(256) k_reclaim(device_tree T, uint32_t M) {
-  control_block* c              = T.ctl;
-  const unsigned long long head = c->retire_head;
-  unsigned long long n          = c->retire_tail - head;
+  auto warp                       = cg::tiled_partition<32>(cg::this_thread_block());
+  control_block* c                = T.ctl;
+  const unsigned long long head   = c->retire_head;
+  unsigned long long n            = c->retire_tail - head;
   if (n > c->reclaim_cap) n = c->reclaim_cap;
   if (M == mvbt::kReclaimAll) M = c->epoch;
-  uint32_t* ring                  = reinterpret_cast<uint32_t*>(c->free_ring);
-  const unsigned long long tail   = c->free_tail;
   const uint32_t lane             = threadIdx.x & 31u;
   const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
   // b is the same in every lane of a warp, so every lane takes the same number of iterations
@@ -105,25 +104,14 @@ __global__ void __launch_bounds__(256) k_reclaim(device_tree T, uint32_t M) {
     const unsigned long long i = b + lane;
     uint32_t idx               = mvbt::kNone;
     const int r                = i < n ? T.reclaim_entry(head + i, M, idx) : 0;
-    const uint32_t fm          = __ballot_sync(0xFFFFFFFFu, r == 1);
-    uint32_t first             = 0;
-    if (lane == 0 && fm) first = atomicAdd(&c->rc_pending, (uint32_t)__popc(fm));
-    first = __shfl_sync(0xFFFFFFFFu, first, 0);
-    if (r == 1) ring[(tail + first + __popc(fm & ((1u << lane) - 1u))) & (c->ring_cap - 1u)] = idx;
+    mvbt::ring_push(c, r == 1, idx, warp);
     if (r == 2) atomicMin(&c->rc_first_kept, (uint32_t)i);
   }
 }
 
-// End of a reclaim pass: one block of kMaxSmSlots threads.
+// End of a reclaim pass: moves the log head (one thread).
 __global__ void k_reclaim_finish(device_tree T) {
-  __shared__ uint32_t freed;
-  control_block* c = T.ctl;
-  if (threadIdx.x == 0) freed = c->rc_pending;
-  __syncthreads();
-  const unsigned long long tail = c->free_tail;
-  T.reclaim_return_chunk((int)threadIdx.x, tail, [&](uint32_t k) { return atomicAdd(&c->rc_pending, k); });
-  __syncthreads();
-  if (threadIdx.x == 0) T.reclaim_publish(c->rc_pending, freed);
+  if (threadIdx.x == 0) T.reclaim_publish();
 }
 
 __global__ void k_snapshot(control_block* c, uint32_t* out) {
@@ -595,6 +583,13 @@ int mvbt_create(int kind, const mvbt_config* cfg_in, mvbt_tree** out) {
       mvbt_destroy(t);
       return fail(MVBT_ERR_OUT_OF_MEMORY, "cudaMalloc of the reclamation rings failed");
     }
+    // both start empty: every slot all ones (kRingEmpty; an index >= capacity in the log)
+    if (cudaMemset(t->retire_log, 0xFF, (uint64_t)log_cap * 4) != cudaSuccess ||
+        cudaMemset(t->free_ring, 0xFF, (uint64_t)ring_cap * 4) != cudaSuccess) {
+      cudaGetLastError();
+      mvbt_destroy(t);
+      return fail(MVBT_ERR_CUDA, "cudaMemset of the reclamation rings failed");
+    }
   }
   k_init<<<1, 256>>>(t->pool, t->ctl, (uint32_t)capacity, t->chunk, t->spin_limit, t->wait_ms * 1000000u,
                      t->retire_log, t->free_ring, log_cap, ring_cap);
@@ -1051,8 +1046,11 @@ namespace {
 constexpr uint32_t kLoadFill = 10;
 constexpr uint32_t kLoadMin  = 1u << 12;  // smaller inserts into a pristine tree go key by key
 
+// Scratch of a bulk load after the sort's own: keep[n] | scan sums | the plan. Every region starts
+// on a 64-word (256-byte) boundary: the plan holds 64-bit fields, and n may be odd.
+inline uint64_t round64(uint64_t words) { return (words + 63) & ~63ull; }
 uint64_t bulk_load_extra_words(uint32_t n) {
-  return (uint64_t)n + ((mvbt_sort::scan_scratch_words(n) + 63) & ~63ull) + (sizeof(bulk_plan) + 255) / 4;
+  return round64(n) + round64(mvbt_sort::scan_scratch_words(n)) + round64((sizeof(bulk_plan) + 3) / 4);
 }
 
 // Insert of a sorted call into a pristine tree: the last occurrence of every key, compacted, built
@@ -1062,8 +1060,8 @@ int bulk_load_sorted(mvbt_tree* t, const sorted_ops& so, const uint32_t* values,
   uint32_t* ck   = so.keys + 2ull * n;  // the sort's ping-pong buffers are free again
   uint32_t* cv   = so.keys + 3ull * n;
   uint32_t* keep = so.extra;
-  uint32_t* sums = so.extra + n;
-  auto* plan     = reinterpret_cast<bulk_plan*>(so.extra + n + ((mvbt_sort::scan_scratch_words(n) + 63) & ~63ull));
+  uint32_t* sums = so.extra + round64(n);
+  auto* plan     = reinterpret_cast<bulk_plan*>(sums + round64(mvbt_sort::scan_scratch_words(n)));
   const unsigned grid = (unsigned)std::min<uint64_t>(((uint64_t)n + 255) / 256, (uint64_t)t->num_sms * 16);
   k_keep_flags<<<grid, 256, 0, s>>>(so.keys, n, keep);
   if (mvbt_sort::exclusive_scan(keep, n, sums, s)) return check_launch();
@@ -1280,7 +1278,7 @@ int mvbt_reclaim(mvbt_tree* t, uint32_t min_live_snapshot, void* stream) {
   k_reclaim<<<(unsigned)t->num_sms * 4u, 256, 0, s>>>(t->view(), min_live_snapshot);
   int st = check_launch();
   if (st) return st;
-  k_reclaim_finish<<<1, mvbt::kMaxSmSlots, 0, s>>>(t->view());
+  k_reclaim_finish<<<1, 32, 0, s>>>(t->view());
   return check_launch();
 }
 
@@ -1363,9 +1361,8 @@ int mvbt_stats(mvbt_tree* t, uint64_t* out, uint32_t n) {
   for (int i = 0; i < 16; ++i) v[6 + i] = c.err_site[i];
   v[22] = c.stat_restarts;
   v[23] = c.stat_reclaimed;
-  const unsigned long long fh = c.ring_fail < c.free_head ? c.ring_fail : c.free_head;
-  v[24] = rc ? c.free_tail - fh : 0;
-  v[25] = c.stat_reused + (rc ? fh - c.free_mark : 0);
+  v[24] = rc ? (uint64_t)std::max<long long>(0, (long long)c.free_avail) : 0;
+  v[25] = mvbt::stat_total(c, 2);
   v[26] = c.stat_log_dropped;
   for (int i = 0; i < 16; ++i) v[27 + i] = c.err_site[16 + i];
   for (uint32_t i = 0; i < n && i < 43; ++i) out[i] = v[i];

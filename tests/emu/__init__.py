@@ -36,7 +36,7 @@ def lib():
             "emu_batch_run": (None, [vp, u32, np.ctypeslib.ndpointer(dtype=np.uint64, flags="C_CONTIGUOUS"),
                                      u32p, u32p, u32p,
                                      np.ctypeslib.ndpointer(dtype=np.uint64, flags="C_CONTIGUOUS"),
-                                     u32p, u32p, vp, i, i, i]),
+                                     u32p, u32p, vp, i, i, i, i, u32, vp]),
         }
         for name, (res, args) in sig.items():
             f = getattr(_lib, name)
@@ -140,12 +140,15 @@ class EmuTree:
                                 counts.ctypes.data, avg_len, self.tiles, self.W)
         return pairs[: lo.size], counts[: lo.size]
 
-    def run_batches(self, b, mode: int = 0):
-        """Runs workload.Batches; returns (result, range_out words)."""
+    def run_batches(self, b, mode: int = 0, reclaim: bool = False, watermark: int = 0xFFFFFFFF,
+                    series=None):
+        """Runs workload.Batches; returns (result, range_out words). reclaim: reclamation inside the
+        persistent run (series: a uint64 array [num_batches, 4] for the memory samples)."""
         result = np.zeros(b.num_ops, np.uint32)
         out = np.full(max(1, b.range_pairs) * 2, 0xFFFFFFFF, np.uint32)
         self.L.emu_batch_run(self.h, b.num_batches, b.batch_off, b.type, b.key, b.arg, b.out_off,
-                             b.range_cap, result, out.ctypes.data, mode, self.tiles, self.W)
+                             b.range_cap, result, out.ctypes.data, mode, self.tiles, self.W,
+                             int(reclaim), watermark, series.ctypes.data if series is not None else None)
         return result, out
 
     def validate(self, ts=0xFFFFFFFF) -> dict:

@@ -129,8 +129,8 @@ void* emu_create(int versioned, uint32_t capacity, uint32_t spin_limit, uint32_t
     };
     log_cap  = pow2(capacity);
     ring_cap = pow2((uint64_t)capacity + (uint64_t)mvbt::kMaxSmSlots * chunk);
-    t->retire_log.assign(log_cap, 0xA5A5A5A5u);
-    t->free_ring.assign(ring_cap, 0xA5A5A5A5u);
+    t->retire_log.assign(log_cap, 0xFFFFFFFFu);  // both start empty, as mvbt_create fills them
+    t->free_ring.assign(ring_cap, 0xFFFFFFFFu);
   }
   mvbt::init_control(t->ctl, capacity, chunk, spin_limit ? spin_limit : (1u << 20), 4000u * 1000u * 1000u,
                      reclaim ? (unsigned long long)t->retire_log.data() : 0ull,
@@ -144,23 +144,20 @@ void emu_reclaim(void* h, uint32_t M) {
   auto v  = t->view();
   auto& c = t->ctl;
   if (M == mvbt::kReclaimAll) M = c.epoch;
-  const unsigned long long head = c.retire_head, tail = c.free_tail;
+  const unsigned long long head = c.retire_head;
   const unsigned long long n    = std::min<unsigned long long>(c.retire_tail - head, c.reclaim_cap);
   uint32_t* ring                = reinterpret_cast<uint32_t*>(c.free_ring);
   for (unsigned long long i = 0; i < n; ++i) {
     uint32_t idx = 0;
     const int r  = v.reclaim_entry(head + i, M, idx);
-    if (r == 1) ring[(tail + c.rc_pending++) & (c.ring_cap - 1u)] = idx;
+    if (r == 1) {  // the ring push of one lane: reserve, write, publish
+      ring[c.free_tail++ & (c.ring_cap - 1u)] = idx;
+      c.free_avail += 1;
+      c.stat_reclaimed += 1;
+    }
     if (r == 2) c.rc_first_kept = std::min<uint32_t>(c.rc_first_kept, (uint32_t)i);
   }
-  const uint32_t freed = c.rc_pending;
-  for (int s = 0; s < mvbt::kMaxSmSlots; ++s)
-    v.reclaim_return_chunk(s, tail, [&](uint32_t k) {
-      const uint32_t o = c.rc_pending;
-      c.rc_pending += k;
-      return o;
-    });
-  v.reclaim_publish(c.rc_pending, freed);
+  v.reclaim_publish();
 }
 
 void emu_destroy(void* h) { delete static_cast<emu_tree*>(h); }
@@ -177,9 +174,8 @@ void emu_stats(void* h, uint64_t* out) {
   out[20] = c.stat_restarts;
   out[21] = c.reclaim_cap ? c.retire_tail : mvbt::stat_total(c, 0);
   out[22] = c.stat_reclaimed;
-  const unsigned long long fh = c.ring_fail < c.free_head ? c.ring_fail : c.free_head;
-  out[23] = c.reclaim_cap ? c.free_tail - fh : 0;
-  out[24] = c.stat_reused + (c.reclaim_cap ? fh - c.free_mark : 0);
+  out[23] = c.reclaim_cap ? (uint64_t)std::max<long long>(0, (long long)c.free_avail) : 0;
+  out[24] = mvbt::stat_total(c, 2);
   out[25] = c.stat_log_dropped;
 }
 
@@ -326,9 +322,12 @@ void emu_find_erase(void* h, const uint32_t* fkeys, uint32_t* out, uint64_t n_fi
 
 // Mixed batches. mode 0: the persistent worker loop (claim order writes-first per batch, batch b
 // waits for the writes of batch b - 1); mode 1: one snapshot + one run per batch.
+// reclaim = 1: reclamation inside the persistent run (mvbt_batch_plan_set_reclaim) with external
+// watermark ext; series (nullable) receives 4 values per batch as mvbt_batch_plan_memory_series.
 void emu_batch_run(void* h, uint32_t nb, const uint64_t* off, const uint32_t* type, const uint32_t* key,
                    const uint32_t* arg, const uint64_t* out_off, const uint32_t* cap, uint32_t* result,
-                   uint32_t* range_out, int mode, int tiles, int W) {
+                   uint32_t* range_out, int mode, int tiles, int W, int reclaim, uint32_t ext,
+                   uint64_t* series) {
   auto* t = static_cast<emu_tree*>(h);
   auto v  = t->view();
   mvbt::batch_view B{type, key, arg, out_off, cap, result, reinterpret_cast<uint2*>(range_out)};
@@ -357,13 +356,27 @@ void emu_batch_run(void* h, uint32_t nb, const uint64_t* off, const uint32_t* ty
   }
   unsigned long long cursors[2] = {0, 0};
   uint32_t done                 = 0;
-  uint32_t params[2]            = {nb, t->ctl.epoch};
+  uint32_t params[3]            = {nb, t->ctl.epoch, ext};
   mvbt::batch_sched sc{off, perm.data(), n_writes.data(), wpre.data(), rpre.data(), writes_done.data(),
                        &done, &cursors[0], &cursors[1], params};
+  std::vector<uint32_t> reads_done(nb, 0);
+  std::vector<unsigned long long> tail_at(nb, ~0ull), ser(4ull * nb, 0);
+  uint32_t full_done           = 0;
+  unsigned long long rc_limit  = 0;
+  if (reclaim && t->ctl.reclaim_cap) {  // as k_batch_begin_reclaim
+    const uint32_t S0 = params[1];
+    rc_limit      = (ext == mvbt::kReclaimAll || S0 <= ext) ? t->ctl.retire_tail : t->ctl.retire_head;
+    sc.reads_done = reads_done.data();
+    sc.full_done  = &full_done;
+    sc.tail_at    = tail_at.data();
+    sc.rc_limit   = &rc_limit;
+    sc.series     = ser.data();
+  }
   EMU_DISPATCH(W, run_warps(std::max(1, tiles * kW / 32), kW, [&](const emu_tile& warp, const emu_tile& tile) {
     mvbt::batched_worker<kW>(v, B, sc, warp, tile);
   }));
   t->ctl.epoch = params[1] + nb;
+  if (series && sc.series) std::memcpy(series, ser.data(), ser.size() * sizeof(uint64_t));
 }
 
 int emu_validate(void* h, uint32_t ts, mvbt_report* rep) {

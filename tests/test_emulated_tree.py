@@ -218,3 +218,49 @@ def test_emulated_sorted_runs_match_oracle(w):
         assert np.array_equal(pairs[mask], ep[mask]), ts
     rep = t.validate()
     assert rep["violations"] == 0 and rep["locked_nodes"] == 0 and rep["keys"] == m.size()
+
+
+@pytest.mark.parametrize("w", [8, 16])
+def test_emulated_reclamation_inside_persistent_runs(w):
+    """Reclamation inside the persistent batched run: idle warps free the copies that no snapshot
+    reads any more, and the run's own writes allocate them again. Results stay identical to the
+    oracle's, the node high-water mark stays well below a run without reclamation, and the memory
+    samples count freed nodes. Then a snapshot held outside the runs (the watermark) stays exact
+    while later runs go on."""
+    from emu import EmuTree
+    import workload as wl
+    import oracle
+    seed, n0 = 17, 3000
+    init = wl.distinct_keys(seed, 0, n0)
+    vals = wl.values_for(init, 0)
+    trees = {}
+    for rc in (False, True):
+        trees[rc] = EmuTree(True, capacity=1 << 15, tiles=8, W=w, reclaim=True)
+        trees[rc].insert(init, vals)
+    m = oracle.MVMap(True)
+    m.insert(init, vals)
+    gen = wl.MixGenerator(seed, n0, stride=wl.stride_for(n0), fixed_batch=96)
+    held = None
+    for rnd in range(8):
+        if rnd == 5:  # from here on the caller reads this snapshot outside the runs
+            held = trees[True].snapshot(); trees[False].snapshot(); m.take_snapshot()
+        b = gen.generate(24)
+        er, eo = m.run_batches(b)
+        series = np.zeros((24, 4), np.uint64)
+        for rc, t in trees.items():
+            r, o = t.run_batches(b, reclaim=rc, watermark=0xFFFFFFFF if held is None else held,
+                                 series=series if rc else None)
+            assert t.errors == 0
+            assert np.array_equal(r, er), (rnd, rc, np.count_nonzero(r != er))
+            assert np.array_equal(o, eo), (rnd, rc)
+        assert np.all(series[:, 0] == np.arange(24) + series[0, 0])  # epochs of the batches' writes
+        assert np.all(np.diff(series[:, 3].astype(np.int64)) >= 0)  # nodes freed so far: monotone
+        if rnd == 4:
+            st = trees[True].stats()
+            assert st["reclaimed"] > 0 and st["reused"] > 0, st
+            assert trees[True].bump < trees[False].bump, (trees[True].bump, trees[False].bump)
+    q = np.concatenate([init, wl.distinct_keys(seed, wl.MISS_INDEX_BASE, 300)])
+    assert np.array_equal(trees[True].find(q, held), m.find(q, held))
+    for t in trees.values():
+        rep = t.validate()
+        assert rep["violations"] == 0 and rep["locked_nodes"] == 0 and rep["keys"] == m.size()

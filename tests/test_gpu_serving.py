@@ -181,3 +181,41 @@ def test_serving_rejects_bad_traces(torch):
         t.serve(b, arrival, reclaim_every=1)  # the tree was made without reclaim
     with pytest.raises(mv.MVBTError):
         t.serve(b, arrival, max_ops_per_launch=1)  # a request is larger than a launch
+
+
+@pytest.mark.parametrize("w", [8, 16])
+def test_serving_with_reclamation_inside_launches_and_lag_admission(torch, w):
+    """Serving with reclamation inside every launch (reclaim_in_launch) and admission by
+    reclamation lag (max_reclaim_lag): results are identical to the oracle with the same groups
+    applied as batches, copies are freed and reused during the session, the lag limit defers
+    admissions, and the node high-water mark stays below a session that keeps every version."""
+    import workload as wl
+    import mvgpubtree_b200 as mv
+    import oracle
+    initial, seed, R = 100_000, 93, 2000
+    b, arrival = wl.serving_trace(seed, initial, R, offered_mops=40.0, stride=wl.stride_for(initial),
+                                  batch_max=8192, erase_lag=128)
+    outs, stats = {}, {}
+    for name, kw in (("keep", {}), ("inside", {"reclaim_in_launch": 1, "max_reclaim_lag": 20000})):
+        t, init = make_tree(torch, mv, wl, initial, seed, w, reclaim=bool(kw))
+        outs[name] = t.serve(b, arrival, max_requests_per_launch=64, **kw)
+        assert t.check_errors() == 0
+        stats[name] = (outs[name]["stats"], t.stats(), t.compute_memory_usage()["nodes_allocated"])
+        rep = t.validate_tree_structure()
+        assert rep["violations"] == 0 and rep["locked_nodes"] == 0
+    for name, out in outs.items():
+        snaps = out["snapshot"].astype(np.int64)
+        steps = np.diff(snaps)
+        starts = np.concatenate([[0], np.nonzero(steps)[0] + 1, [R]])
+        m = oracle.MVMap(True)
+        m.insert(init, wl.values_for(init, 0))
+        g = wl.Batches(b.batch_off[starts].astype(np.uint64), b.type, b.key, b.arg, b.out_off,
+                       b.range_cap, b.range_pairs)
+        er, eo = m.run_batches(g)
+        find = b.type == 0
+        assert np.array_equal(out["result"][find], er[find]), name
+        assert range_views(b, out["result"], out["range_out"]) == range_views(b, er, eo.reshape(-1, 2)), name
+    sv, tr, nodes = stats["inside"]
+    assert tr["reclaimed"] > 0 and tr["reused"] > 0, tr
+    assert sv["max_reclaim_lag"] > 0 and sv["nodes_high_water"] > 0
+    assert nodes < stats["keep"][2], (nodes, stats["keep"][2])
