@@ -979,6 +979,8 @@ struct device_tree {
     uint32_t n             = 0;
     if (warp.thread_rank() == 0) {
       h = ld_relaxed_u64(&c->retire_head);
+      const unsigned long long tail = ld_relaxed_u64(&c->retire_tail);
+      if (limit > tail) limit = tail;  // never past the entries reserved so far
       if (h < limit) {
         n = (uint32_t)(limit - h < 32 ? limit - h : 32);
         if (atomicCAS(&c->retire_head, h, h + n) != h) n = 0;  // another warp took them
@@ -1852,21 +1854,14 @@ MVBT_DEV bool reclaim_step(const device_tree& T, const batch_sched& sc, uint32_t
   lim = warp.shfl(lim, 0);
   return T.reclaim_online(lim, warp) > 0;
 }
-// At the end of a warp's work: reclaim while there is reclaimable work, bounded by the wait limit
-// (the last batches' reads may still be running in other warps; what is left waits for the next
-// launch or a pass between launches).
+// At the end of a warp's work: one more reclamation step (at most 32 copies), then leave. The
+// copies the last batches made become reclaimable only when their last reads finish, at the very
+// end of the launch, when few warps are left; draining them there would stretch the launch, so
+// they wait for the next launch, whose warps free them from its start while work runs.
 template <class Warp>
 MVBT_DEV void reclaim_drain(const device_tree& T, const batch_sched& sc, uint32_t nb, const Warp& warp) {
-  const unsigned long long t0 = global_ns();
-  for (uint32_t idle = 0; idle < 4 && !wait_expired(t0, T.ctl->wait_ns, warp);) {
-    if (warp.thread_rank() == 0) advance_done(sc, nb, T.ctl);
-    if (reclaim_step(T, sc, nb, warp)) {
-      idle = 0;
-    } else {
-      ++idle;
-      __nanosleep(512);
-    }
-  }
+  if (warp.thread_rank() == 0) advance_done(sc, nb, T.ctl);
+  reclaim_step(T, sc, nb, warp);
 }
 
 // Worker loop of one warp in the persistent batched launch. The warp claims consecutive claim
@@ -1934,6 +1929,9 @@ MVBT_DEV void batched_worker(const device_tree& T, const batch_view& B, const ba
           // advance done_batches.
           if (t.thread_rank() == 0) atomicAdd(&sc.writes_done[b], 1u);
         }
+        // the writes just made copies: free as many older ones as there are reclaimable, so
+        // that reclamation keeps pace with copying even when no warp is ever idle
+        if (did && sc.rc_limit) reclaim_step(T, sc, nb, warp);
       }
     }
     if (!did && r < TR) {
@@ -1945,8 +1943,9 @@ MVBT_DEV void batched_worker(const device_tree& T, const batch_view& B, const ba
         did = r0 < TR;
         uint32_t b = rb, dd = d;
         uint32_t done_b[kReadClaim];  // batch of each read this tile ran (counted after a fence)
+#pragma unroll
+        for (uint32_t k = 0; k < kReadClaim; ++k) done_b[k] = 0xFFFFFFFFu;  // all set: the loop may stop early
         for (uint32_t k = 0; k < kReadClaim; ++k) {
-          done_b[k]                  = 0xFFFFFFFFu;
           const unsigned long long x = r0 + k * kTiles + tid;
           if (x >= TR) break;
           b = batch_of_ordinal(sc.rpre, nb, x, b);
@@ -1967,7 +1966,7 @@ MVBT_DEV void batched_worker(const device_tree& T, const batch_view& B, const ba
           t.sync();
           if (t.thread_rank() == 0)
             for (uint32_t k = 0; k < kReadClaim; ++k)
-              if (done_b[k] != 0xFFFFFFFFu) atomicAdd(&sc.reads_done[done_b[k]], 1u);
+              if (done_b[k] < nb) atomicAdd(&sc.reads_done[done_b[k]], 1u);
         }
       }
     }
