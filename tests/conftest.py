@@ -26,4 +26,8 @@ def _built_libraries():
     build_workload()
     from oracle.build import build as build_oracle
     build_oracle()
+    spec = importlib.util.spec_from_file_location("cpp_build", ROOT / "tests" / "cpp" / "build.py")
+    cpp = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(cpp)
+    cpp.build_user_kernels()
     yield
