@@ -416,6 +416,31 @@ struct header {
   MVBT_DEV bool is_leaf() const { return level() == 0; }
 };
 
+// Every lane loads the header words (26..31) of the node at p itself: read-only cached loads, for
+// readers that run with no writer in flight. They read the 128-byte line the lane's own share
+// comes from, so they cost two L1 accesses where get_header costs six shuffles.
+#if defined(MVBT_HOST_EMULATION)
+MVBT_DEV header ld_header_words(const uint32_t* p) {
+  header h;
+  h.low  = __atomic_load_n(p + 26, __ATOMIC_RELAXED);
+  h.mod  = __atomic_load_n(p + 27, __ATOMIC_RELAXED);
+  h.high = __atomic_load_n(p + 28, __ATOMIC_RELAXED);
+  h.link = __atomic_load_n(p + 29, __ATOMIC_RELAXED);
+  h.ts   = __atomic_load_n(p + 30, __ATOMIC_RELAXED);
+  h.ol   = __atomic_load_n(p + 31, __ATOMIC_RELAXED);
+  return h;
+}
+#else
+MVBT_DEV header ld_header_words(const uint32_t* p) {
+  header h;
+  asm("ld.global.nc.v2.u32 {%0,%1}, [%2];" : "=r"(h.low), "=r"(h.mod) : "l"(p + 26));
+  asm("ld.global.nc.v4.u32 {%0,%1,%2,%3}, [%4];"
+      : "=r"(h.high), "=r"(h.link), "=r"(h.ts), "=r"(h.ol)
+      : "l"(p + 28));
+  return h;
+}
+#endif
+
 MVBT_DEV header make_header(uint32_t low, uint32_t mod, uint32_t high, uint32_t link, uint32_t ts,
                             uint32_t ol) {
   header h;
@@ -1129,6 +1154,48 @@ struct device_tree {
     return kNotFound;
   }
 
+  // The point lookup of a tree no writer changes meanwhile (concurrent = false): the same route
+  // and result as cooperative_find(key, t, ts, false, start, f), but every lane loads the header
+  // words itself (ld_header_words) beside its share of the node instead of receiving them by
+  // shuffle, and the versions a snapshot read passes over are read as headers alone.
+  template <int W, class Tile>
+  MVBT_DEV uint32_t find_quiescent(uint32_t key, const Tile& t, uint32_t ts = kLatest, uint32_t start = kAnchor,
+                                   finger<W>* f = nullptr) const {
+    const bool snap = versioned && ts != kLatest;
+    uint32_t idx    = start;
+    node_regs<W> n;
+    for (uint32_t step = 0; step < kMaxSteps; ++step) {
+      if (!valid(idx, t)) return kNotFound;
+      const header h = ld_header_words(node_ptr(idx));
+      load<W>(idx, n, false, t);  // issued with the header loads: one round trip per visit
+      if (snap && h.ts > ts) {  // a newer version: move to the older one
+        idx = h.older();
+        if (idx == kNone) {
+          if (t.thread_rank() == 0) set_error(kErrCorrupt, 3);
+          return kNotFound;
+        }
+        continue;
+      }
+      if (key < h.low) {
+        idx = kAnchor;
+        continue;
+      }
+      if (key >= h.high && h.sibling() != kNone) {
+        idx = h.sibling();
+        continue;
+      }
+      if (h.is_leaf()) {
+        if (f) f->record(0, idx, h.low, h.high, t);
+        return leaf_value<W>(n, key, t);
+      }
+      if (f) f->record(h.level(), idx, h.low, h.high, t);
+      idx = child_for<W>(n, key, t);
+      if (idx == kNone) idx = kAnchor;
+    }
+    if (t.thread_rank() == 0) set_error(kErrStepLimit, 4);
+    return kNotFound;
+  }
+
   // ------------------------------------------------------------------------------------------
   // Range query [lo, hi) at snapshot ts. Writes at most cap pairs {key, value} ascending at out
   // (nullable) and returns the full count.
@@ -1300,6 +1367,66 @@ struct device_tree {
     if (leaf == kNone) return false;
     return insert_at<W>(key, value, t, E, leaf, f.idx, kNone, (uint32_t)W - 1);
   }
+
+  // Inserts the keys of a sorted run that land in one leaf under a single lock (the sorted batch
+  // front-end): skeys[i] ascending, its value at values[spos[i]]. The leaf of skeys[i] is locked
+  // and prepared for epoch E once; then that key and each following key of the run below the
+  // leaf's high fence is merged into the node in registers while the leaf has room, and the leaf
+  // is stored and released once. A key that finds the leaf full splits it (split_insert), its
+  // separators go up as in insert_at, and the group ends there. Keys repeated in the run count at
+  // their last occurrence only (i + 1 < n_all with the same key: skipped); the caller starts a
+  // group at such a last occurrence. Advances i past every key the group consumed (at least one).
+  template <int W, class Tile>
+  MVBT_DEV void insert_run_group(const uint32_t* skeys, const uint32_t* spos, const uint32_t* values,
+                                 uint64_t& i, uint64_t end, uint64_t n_all, const Tile& t, uint32_t E,
+                                 finger<W>& f) const {
+    uint32_t key = skeys[i];
+    if (key == kEmptyKey) {  // not a key; the run is sorted, so every later one is the same
+      i = end;
+      return;
+    }
+    node_regs<W> n;
+    header h;
+    uint32_t leaf = descend_with_finger<W>(key, f, t);
+    if (leaf != kNone) leaf = lock_covering<W>(leaf, 0, key, n, h, t);
+    if (leaf == kNone) {
+      ++i;
+      return;
+    }
+    if (!prepare_write<W>(leaf, n, h, E, t)) {
+      unlock(leaf, t);
+      ++i;
+      return;
+    }
+    int nvalid = count_valid<W>(n, t);
+    for (;;) {
+      const uint32_t value = values[spos[i]];
+      ++i;
+      const int pos = find_pos<W>(n, key, t);
+      if (pos >= 0) {
+#pragma unroll
+        for (int j = 0; j < 16 / W; ++j)
+          if (pair_index<W>(t, j) == pos) n.v[j] = value;
+      } else if (nvalid < kDataPairs) {
+        node_regs<W> out;
+        build_from_merged<W>(n, count_less<W>(n, key, t), key, value, 0, nvalid + 1, out, t);
+        n = out;
+        ++nvalid;
+      } else {  // full: split with this key (stores the node, releases it) and end the group
+        uint32_t sep_key = 0, sep_child = kNone;
+        if (split_insert<W>(leaf, n, h, key, value, E, sep_key, sep_child, t))
+          push_up<W>(sep_key, sep_child, E, f.idx, kNone, (uint32_t)W - 1, t);
+        return;
+      }
+      while (i < end && i + 1 < n_all && skeys[i + 1] == skeys[i]) ++i;
+      if (i >= end) break;
+      key = skeys[i];
+      if (key >= h.high || key == kEmptyKey) break;
+    }
+    store<W>(leaf, n, t);
+    release(leaf, h, t);
+  }
+
   template <int W, class Tile>
   MVBT_DEV bool erase_in_run(uint32_t key, const Tile& t, uint32_t E, finger<W>& f) const {
     if (key == kEmptyKey) return false;
@@ -1559,41 +1686,53 @@ struct device_tree {
       // full leaf: split, then push separators up
       uint32_t sep_key = 0, sep_child = kNone;
       if (!split_insert<W>(leaf, n, h, key, value, E, sep_key, sep_child, t)) return false;
-      uint32_t level = 1;
-      while (sep_child != kNone) {
-        uint32_t start;
-        if (level <= top) {
-          start = (level < (uint32_t)W) ? t.shfl(path0, level) : t.shfl(path1, level - W);
-          if (start == kNone) start = kAnchor;
-        } else {
-          start = kAnchor;
-        }
-        if (level >= (uint32_t)kMaxLevels) {
-          if (t.thread_rank() == 0) set_error(kErrCorrupt, 13);
-          return false;
-        }
-        uint32_t p = lock_covering<W>(start, level, sep_key, n, h, t);
-        if (p == kNone) return false;
-        if (!prepare_write<W>(p, n, h, E, t)) {
-          unlock(p, t);
-          return false;
-        }
-        if (p == kAnchor) return grow<W>(n, h, sep_key, sep_child, E, t);
-        nvalid = count_valid<W>(n, t);
-        if (nvalid < kDataPairs) {
-          int ipos = count_less<W>(n, sep_key, t);
-          node_regs<W> out;
-          build_from_merged<W>(n, ipos, sep_key, sep_child, 0, nvalid + 1, out, t);
-          store<W>(p, out, t);
-          release(p, h, t);
-          return true;
-        }
-        uint32_t k2 = sep_key, c2 = sep_child;
-        if (!split_insert<W>(p, n, h, k2, c2, E, sep_key, sep_child, t)) return false;
-        ++level;
-      }
-      return true;
+      return push_up<W>(sep_key, sep_child, E, path0, path1, top, t);
     }
+  }
+
+  // Inserts the separator {sep_key -> sep_child} of a leaf split into the level above, splitting
+  // full interior nodes in turn and growing the tree at the anchor. path0 / path1 / top are the
+  // parent hints as descend_for_write records them.
+  template <int W, class Tile>
+  MVBT_DEV bool push_up(uint32_t sep_key, uint32_t sep_child, uint32_t E, uint32_t path0, uint32_t path1,
+                        uint32_t top, const Tile& t) const {
+    node_regs<W> n;
+    header h;
+    int nvalid;
+    uint32_t level = 1;
+    while (sep_child != kNone) {
+      uint32_t start;
+      if (level <= top) {
+        start = (level < (uint32_t)W) ? t.shfl(path0, level) : t.shfl(path1, level - W);
+        if (start == kNone) start = kAnchor;
+      } else {
+        start = kAnchor;
+      }
+      if (level >= (uint32_t)kMaxLevels) {
+        if (t.thread_rank() == 0) set_error(kErrCorrupt, 13);
+        return false;
+      }
+      uint32_t p = lock_covering<W>(start, level, sep_key, n, h, t);
+      if (p == kNone) return false;
+      if (!prepare_write<W>(p, n, h, E, t)) {
+        unlock(p, t);
+        return false;
+      }
+      if (p == kAnchor) return grow<W>(n, h, sep_key, sep_child, E, t);
+      nvalid = count_valid<W>(n, t);
+      if (nvalid < kDataPairs) {
+        int ipos = count_less<W>(n, sep_key, t);
+        node_regs<W> out;
+        build_from_merged<W>(n, ipos, sep_key, sep_child, 0, nvalid + 1, out, t);
+        store<W>(p, out, t);
+        release(p, h, t);
+        return true;
+      }
+      uint32_t k2 = sep_key, c2 = sep_child;
+      if (!split_insert<W>(p, n, h, k2, c2, E, sep_key, sep_child, t)) return false;
+      ++level;
+    }
+    return true;
   }
 
   // Erase key in write epoch E. Returns true if the key was present.

@@ -137,7 +137,7 @@ __global__ void __launch_bounds__(256) k_find(device_tree T, const uint32_t* __r
   auto tile = cg::tiled_partition<W>(cg::this_thread_block());
   for (uint64_t i = first_tile<W>(); i < n; i += num_tiles<W>()) {
     uint32_t key = keys[i];
-    uint32_t v   = T.cooperative_find<W>(key, tile, ts, kStrong);
+    uint32_t v   = kStrong ? T.cooperative_find<W>(key, tile, ts, true) : T.find_quiescent<W>(key, tile, ts);
     if (tile.thread_rank() == 0) out[i] = v;
   }
 }
@@ -255,7 +255,8 @@ __global__ void __launch_bounds__(256) k_find_sorted(device_tree T, const uint32
   mvbt::finger<W> f;
   for (; i < end; ++i) {
     const uint32_t key = skeys[i];
-    const uint32_t v   = T.cooperative_find<W>(key, tile, ts, kStrong, f.start_for(key, tile), &f);
+    const uint32_t v   = kStrong ? T.cooperative_find<W>(key, tile, ts, true, f.start_for(key, tile), &f)
+                                 : T.find_quiescent<W>(key, tile, ts, f.start_for(key, tile), &f);
     if (tile.thread_rank() == 0) out[spos[i]] = v;
   }
 }
@@ -294,9 +295,12 @@ __global__ void __launch_bounds__(256) k_insert_sorted(device_tree T, const uint
   uint64_t i, end;
   tile_run<W>(n, i, end);
   mvbt::finger<W> f;
-  for (; i < end; ++i) {
-    if (superseded(skeys, i, n)) continue;
-    T.insert_in_run<W>(skeys[i], values[spos[i]], tile, E, f);
+  while (i < end) {
+    if (superseded(skeys, i, n)) {
+      ++i;
+      continue;
+    }
+    T.insert_run_group<W>(skeys, spos, values, i, end, n, tile, E, f);
   }
 }
 

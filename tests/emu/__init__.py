@@ -26,7 +26,7 @@ def lib():
             "emu_snapshot": (u32, [vp]),
             "emu_insert": (None, [vp, u32p, u32p, u64, i, i]),
             "emu_erase": (None, [vp, u32p, u64, i, i]),
-            "emu_find": (None, [vp, u32p, u32p, u64, u32, i, i]),
+            "emu_find": (None, [vp, u32p, u32p, u64, u32, i, i, i]),
             "emu_range": (None, [vp, u32p, u32p, vp, vp, u32, u64, u32, i, i]),
             "emu_insert_range": (None, [vp, u32p, u32p, u64, u32p, u32p, u64, vp, vp, u32, i, i]),
             "emu_find_erase": (None, [vp, u32p, u32p, u64, u32p, u64, i, i]),
@@ -93,10 +93,10 @@ class EmuTree:
         k = _u32(k)
         self.L.emu_erase(self.h, k, k.size, self.tiles, self.W)
 
-    def find(self, k, ts=0xFFFFFFFF):
+    def find(self, k, ts=0xFFFFFFFF, quiescent=False):
         k = _u32(k)
         out = np.empty_like(k)
-        self.L.emu_find(self.h, k, out, k.size, ts, self.tiles, self.W)
+        self.L.emu_find(self.h, k, out, k.size, ts, self.tiles, self.W, int(quiescent))
         return out
 
     def range(self, lo, hi, avg_len, ts=0xFFFFFFFF):
@@ -111,11 +111,12 @@ class EmuTree:
     def sorted_run(self, kind: str, keys, arg=None, avg_len: int = 0, ts=0xFFFFFFFF):
         """The sorted front-end's kernels on the emulator: keys are sorted here (a stable sort, so a
         repeated key keeps its input order), each tile runs a contiguous share with its path
-        memory, results come back in input order. kind: find | range | insert | erase."""
+        memory, results come back in input order. kind: find | range | insert | erase | qfind (the
+        find of a tree no writer changes meanwhile)."""
         k = _u32(keys)
         order = np.argsort(k, kind="stable").astype(np.uint32)
         sk = np.ascontiguousarray(k[order])
-        code = {"find": 0, "range": 1, "insert": 2, "erase": 3}[kind]
+        code = {"find": 0, "range": 1, "insert": 2, "erase": 3, "qfind": 4}[kind]
         a = _u32(arg) if arg is not None else None
         out = np.zeros(k.size, np.uint32)
         pairs = np.full((max(1, k.size), max(1, avg_len), 2), 0xFFFFFFFF, np.uint32) if kind == "range" else None

@@ -211,12 +211,14 @@ void emu_erase(void* h, const uint32_t* keys, uint64_t n, int tiles, int W) {
   }));
 }
 
-void emu_find(void* h, const uint32_t* keys, uint32_t* out, uint64_t n, uint32_t ts, int tiles, int W) {
+// quiescent != 0: the lookup of a tree no writer changes meanwhile (find_quiescent).
+void emu_find(void* h, const uint32_t* keys, uint32_t* out, uint64_t n, uint32_t ts, int tiles, int W,
+              int quiescent) {
   auto* t = static_cast<emu_tree*>(h);
   auto v  = t->view();
   if (!v.versioned) ts = mvbt::kLatest;
   EMU_DISPATCH(W, run(n, tiles, kW, [&](uint64_t i, const emu_tile& tile) {
-    uint32_t r = v.cooperative_find<kW>(keys[i], tile, ts, true);
+    uint32_t r = quiescent ? v.find_quiescent<kW>(keys[i], tile, ts) : v.cooperative_find<kW>(keys[i], tile, ts, true);
     if (tile.thread_rank() == 0) out[i] = r;
   }));
 }
@@ -258,7 +260,8 @@ void emu_insert_range(void* h, const uint32_t* keys, const uint32_t* vals, uint6
 // Sorted runs (the sorted batch front-end): keys[0, n) ascending, pos[i] = the input position of
 // keys[i]; each of `tiles` tiles takes one contiguous share of the run and keeps its path memory
 // (mvbt::finger, one per lane, as registers are on the GPU). kind: 0 find, 1 range, 2 insert (a
-// repeated key: its last occurrence wins), 3 erase.
+// repeated key: its last occurrence wins; the keys of one leaf under one lock), 3 erase, 4 find of
+// a tree no writer changes meanwhile.
 void emu_sorted_run(void* h, int kind, const uint32_t* keys, const uint32_t* pos, const uint32_t* arg,
                     uint32_t* out, uint32_t* pairs, uint32_t avg_len, uint64_t n, uint32_t ts, int tiles, int W) {
   auto* t = static_cast<emu_tree*>(h);
@@ -281,7 +284,20 @@ void emu_sorted_run(void* h, int kind, const uint32_t* keys, const uint32_t* pos
           const uint64_t b = (uint64_t)x * per, e = std::min<uint64_t>(n, b + per);
           for (uint64_t i = b; i < e; ++i) {
             const uint32_t k = keys[i];
-            if (kind == 0) {
+            if (kind == 2) {
+              while (i < e) {
+                if (i + 1 < n && keys[i + 1] == keys[i]) {
+                  ++i;
+                  continue;
+                }
+                v.insert_run_group<kW>(keys, pos, arg, i, e, n, tile, E, f);
+              }
+              break;
+            }
+            if (kind == 4) {
+              const uint32_t r = v.find_quiescent<kW>(k, tile, ts, f.start_for(k, tile), &f);
+              if (tile.thread_rank() == 0) out[pos[i]] = r;
+            } else if (kind == 0) {
               const uint32_t r = v.cooperative_find<kW>(k, tile, ts, true, f.start_for(k, tile), &f);
               if (tile.thread_rank() == 0) out[pos[i]] = r;
             } else if (kind == 1) {
@@ -289,9 +305,6 @@ void emu_sorted_run(void* h, int kind, const uint32_t* keys, const uint32_t* pos
               const uint32_t c = v.cooperative_range_query<kW>(k, arg[pos[i]], tile, ts, o, avg_len, true,
                                                                f.start_for(k, tile), &f);
               if (out && tile.thread_rank() == 0) out[pos[i]] = c;
-            } else if (kind == 2) {
-              if (i + 1 < n && keys[i + 1] == k) continue;
-              v.insert_in_run<kW>(k, arg[pos[i]], tile, E, f);
             } else {
               v.erase_in_run<kW>(k, tile, E, f);
             }

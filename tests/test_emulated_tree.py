@@ -211,6 +211,8 @@ def test_emulated_sorted_runs_match_oracle(w):
     hi = wl.upper_bounds(lo, 16, wl.stride_for(n0))
     for ts in (s0, s1):
         assert np.array_equal(t.sorted_run("find", q, ts=ts), m.find(q, ts)), ts
+        assert np.array_equal(t.sorted_run("qfind", q, ts=ts), m.find(q, ts)), ts
+        assert np.array_equal(t.find(q, ts, quiescent=True), m.find(q, ts)), ts
         pairs, counts = t.sorted_run("range", lo, hi, avg_len=48, ts=ts)
         ep, ec = m.range_query(lo, hi, 48, ts)
         assert np.array_equal(counts, ec), ts
