@@ -68,6 +68,7 @@
 #include <thread>
 #define MVBT_DEV inline
 #define MVBT_COLD static inline
+#define MVBT_OUTLINE inline
 struct uint2 {
   uint32_t x, y;
 };
@@ -117,6 +118,13 @@ inline thread_local uint32_t sm = 0;  // emulated SM id of the calling lane
 // register count of the persistent kernels past the three-blocks-per-SM limit.
 #ifndef MVBT_COLD
 #define MVBT_COLD __device__ __forceinline__
+#endif
+// The separator push of a split (taken by a minority of writes). Inlined by default, as the
+// persistent kernels need; a translation unit whose kernels are not register-bound defines it as
+// __device__ __noinline__ so that one copy of that code is shared by every call site and the hot
+// loop of a write stays small in the instruction cache.
+#ifndef MVBT_OUTLINE
+#define MVBT_OUTLINE __device__ __forceinline__
 #endif
 #endif
 
@@ -748,10 +756,12 @@ struct finger {
   uint32_t idx  = kNone;
   uint32_t low  = 0;
   uint32_t high = 0;
-  // Lowest remembered node covering key, or the anchor.
+  // Lowest remembered node covering key, or the anchor. level (nullable): that node's level, or
+  // kNone for the anchor.
   template <class Tile>
-  MVBT_DEV uint32_t start_for(uint32_t key, const Tile& t) const {
+  MVBT_DEV uint32_t start_for(uint32_t key, const Tile& t, uint32_t* level = nullptr) const {
     const uint32_t m = t.ballot(idx != kNone && low <= key && key < high);
+    if (level) *level = m ? (uint32_t)(__ffs(m) - 1) : kNone;
     return m ? t.shfl(idx, __ffs(m) - 1) : kAnchor;
   }
   template <class Tile>
@@ -828,7 +838,7 @@ struct device_tree {
     const uint32_t limit          = c->spin_limit;
     const unsigned long long t0 = global_ns();
     for (uint32_t tries = 0; tries < limit; ++tries) {
-      if (ld_relaxed_u32(&c->error) & kErrPoolExhausted) return kNone;
+      if (tries && (ld_relaxed_u32(&c->error) & kErrPoolExhausted)) return kNone;
       unsigned long long old = atomicAdd(slot, 1ull);
       uint32_t base = (uint32_t)(old >> 32), used = (uint32_t)old;
       if (used < C) return base + used;
@@ -1331,11 +1341,14 @@ struct device_tree {
   // Writers
   // ------------------------------------------------------------------------------------------
   // Descent of a writer in a sorted run: like descend_for_write, but it starts at the lowest node
-  // of f covering key and records every node it passes (the leaf at level 0) in f, which then
-  // serves as the path of parent hints (insert_at with path0 = f's per-lane nodes).
+  // of f covering key and records every interior node it passes in f, which then serves as the
+  // path of parent hints (insert_at with path0 = f's per-lane nodes). The leaf is recorded by the
+  // caller once it has read it under its lock.
   template <int W, class Tile>
   MVBT_DEV uint32_t descend_with_finger(uint32_t key, finger<W>& f, const Tile& t) const {
-    uint32_t idx = f.start_for(key, t);
+    uint32_t start_level;
+    uint32_t idx = f.start_for(key, t, &start_level);
+    if (start_level == 0) return idx;  // the leaf of the previous op covers key
     node_regs<W> n;
     for (uint32_t step = 0; step < kMaxSteps; ++step) {
       if (!valid(idx, t)) return kNone;
@@ -1350,9 +1363,14 @@ struct device_tree {
         continue;
       }
       f.record(h.level(), idx, h.low, h.high, t);
-      if (h.is_leaf()) return idx;
-      idx = child_for<W>(n, key, t);
-      if (idx == kNone) idx = kAnchor;
+      if (h.is_leaf()) return idx;  // reached through a sibling link or a misrouted read
+      const uint32_t child = child_for<W>(n, key, t);
+      if (child == kNone) {
+        idx = kAnchor;
+        continue;
+      }
+      if (h.level() == 1) return child;  // a leaf: read under the lock, not before it
+      idx = child;
     }
     if (t.thread_rank() == 0) set_error(kErrStepLimit, 8);
     return kNone;
@@ -1365,7 +1383,7 @@ struct device_tree {
     if (key == kEmptyKey) return false;
     const uint32_t leaf = descend_with_finger<W>(key, f, t);
     if (leaf == kNone) return false;
-    return insert_at<W>(key, value, t, E, leaf, f.idx, kNone, (uint32_t)W - 1);
+    return insert_at<W>(key, value, t, E, leaf, f.idx, kNone, (uint32_t)W - 1, &f);
   }
 
   // Inserts the keys of a sorted run that land in one leaf under a single lock (the sorted batch
@@ -1388,11 +1406,12 @@ struct device_tree {
     node_regs<W> n;
     header h;
     uint32_t leaf = descend_with_finger<W>(key, f, t);
-    if (leaf != kNone) leaf = lock_covering<W>(leaf, 0, key, n, h, t);
+    if (leaf != kNone) leaf = lock_covering<W>(leaf, 0, key, n, h, t, true);
     if (leaf == kNone) {
       ++i;
       return;
     }
+    f.record(0, leaf, h.low, h.high, t);
     if (!prepare_write<W>(leaf, n, h, E, t)) {
       unlock(leaf, t);
       ++i;
@@ -1432,11 +1451,13 @@ struct device_tree {
     if (key == kEmptyKey) return false;
     const uint32_t leaf = descend_with_finger<W>(key, f, t);
     if (leaf == kNone) return false;
-    return erase_at<W>(key, t, E, leaf);
+    return erase_at<W>(key, t, E, leaf, &f);
   }
 
   // Descends to the leaf for key (newest versions, strong loads), recording in `path` the
   // interior node visited at each level: lane l holds level l in path0 and level l + W in path1.
+  // Returns the leaf its level-1 parent names without reading it: the writer reads it under its
+  // lock (lock_covering with direct = true), one round trip instead of three.
   template <int W, class Tile>
   MVBT_DEV uint32_t descend_for_write(uint32_t key, uint32_t& path0, uint32_t& path1,
                                       uint32_t& top_level, const Tile& t) const {
@@ -1473,8 +1494,16 @@ struct device_tree {
       } else {
         if (t.thread_rank() == (int)(lvl - W)) path1 = idx;
       }
-      idx = child_for<W>(n, key, t);
-      if (idx == kNone) idx = kAnchor;
+      const uint32_t child = child_for<W>(n, key, t);
+      if (child == kNone) {
+        idx = kAnchor;
+        continue;
+      }
+      if (lvl == 1) {
+        if (step > 16 && t.thread_rank() == 0) atomicMax(&ctl->stat_max_steps, (unsigned long long)step);
+        return child;
+      }
+      idx = child;
     }
     if (t.thread_rank() == 0) set_error(kErrStepLimit, 8);
     return kNone;
@@ -1522,20 +1551,24 @@ struct device_tree {
 
   // Locks the node at `level` that covers key, starting from idx (the node recorded on the way
   // down, or the anchor). Only a few lock-coupled hops to the right are taken while holding a
-  // lock; a node further right is re-approached unlocked. Returns the locked index with n/h
-  // loaded; kNone on failure.
+  // lock; a node further right is re-approached unlocked. direct: idx is a live node at `level`
+  // named by its parent or recorded on the way down, locked before it is read (a stale or
+  // misrouted one is released again unchanged and approached as above). Returns the locked index
+  // with n/h loaded; kNone on failure.
   template <int W, class Tile>
   MVBT_DEV uint32_t lock_covering(uint32_t idx, uint32_t level, uint32_t key, node_regs<W>& n,
-                                  header& h, const Tile& t) const {
+                                  header& h, const Tile& t, bool direct = false) const {
     for (uint32_t attempt = 0; attempt < kMaxSteps; ++attempt) {
-      idx = seek<W>(idx, level, key, n, h, t);
-      if (idx == kNone) return kNone;
+      if (!direct || attempt > 0) {
+        idx = seek<W>(idx, level, key, n, h, t);
+        if (idx == kNone) return kNone;
+      }
       if (!lock(idx, t)) return kNone;
       load<W>(idx, n, true, t);
       h = get_header<W>(n, t);
       if (h.level() != level || key < h.low) {  // the anchor grew, or the approach was misrouted
         unlock(idx, t);
-        if (key < h.low) idx = kAnchor;
+        if (key < h.low || h.level() < level) idx = kAnchor;
         continue;
       }
       uint32_t hops = 0;
@@ -1647,15 +1680,17 @@ struct device_tree {
   // The insert after its descent: `leaf` and the path (path0 / path1 / top, as descend_for_write
   // records them) may have been found before other writers changed the tree; lock_covering moves
   // right as far as needed and a stale path entry only lengthens the approach to a parent.
+  // f (nullable): path memory of a sorted run, which records the leaf as read under the lock.
   template <int W, class Tile>
   MVBT_DEV bool insert_at(uint32_t key, uint32_t value, const Tile& t, uint32_t E, uint32_t leaf,
-                          uint32_t path0, uint32_t path1, uint32_t top) const {
+                          uint32_t path0, uint32_t path1, uint32_t top, finger<W>* f = nullptr) const {
     if (key == kEmptyKey) return false;
     {
       node_regs<W> n;
       header h;
-      leaf = lock_covering<W>(leaf, 0, key, n, h, t);
+      leaf = lock_covering<W>(leaf, 0, key, n, h, t, true);
       if (leaf == kNone) return false;
+      if (f) f->record(0, leaf, h.low, h.high, t);
       // update in place if present
       int pos = find_pos<W>(n, key, t);
       if (pos >= 0) {
@@ -1694,7 +1729,7 @@ struct device_tree {
   // full interior nodes in turn and growing the tree at the anchor. path0 / path1 / top are the
   // parent hints as descend_for_write records them.
   template <int W, class Tile>
-  MVBT_DEV bool push_up(uint32_t sep_key, uint32_t sep_child, uint32_t E, uint32_t path0, uint32_t path1,
+  MVBT_OUTLINE bool push_up(uint32_t sep_key, uint32_t sep_child, uint32_t E, uint32_t path0, uint32_t path1,
                         uint32_t top, const Tile& t) const {
     node_regs<W> n;
     header h;
@@ -1712,7 +1747,7 @@ struct device_tree {
         if (t.thread_rank() == 0) set_error(kErrCorrupt, 13);
         return false;
       }
-      uint32_t p = lock_covering<W>(start, level, sep_key, n, h, t);
+      uint32_t p = lock_covering<W>(start, level, sep_key, n, h, t, start != kAnchor);
       if (p == kNone) return false;
       if (!prepare_write<W>(p, n, h, E, t)) {
         unlock(p, t);
@@ -1745,14 +1780,16 @@ struct device_tree {
     return erase_at<W>(key, t, E, leaf);
   }
 
-  // The erase after its descent (the leaf may be stale: lock_covering moves right).
+  // The erase after its descent (the leaf may be stale: lock_covering moves right). f (nullable):
+  // as in insert_at.
   template <int W, class Tile>
-  MVBT_DEV bool erase_at(uint32_t key, const Tile& t, uint32_t E, uint32_t leaf) const {
+  MVBT_DEV bool erase_at(uint32_t key, const Tile& t, uint32_t E, uint32_t leaf, finger<W>* f = nullptr) const {
     if (key == kEmptyKey) return false;
     node_regs<W> n;
     header h;
-    leaf = lock_covering<W>(leaf, 0, key, n, h, t);
+    leaf = lock_covering<W>(leaf, 0, key, n, h, t, true);
     if (leaf == kNone) return false;
+    if (f) f->record(0, leaf, h.low, h.high, t);
     int pos = find_pos<W>(n, key, t);
     if (pos < 0) {
       unlock(leaf, t);

@@ -131,11 +131,20 @@ __device__ __forceinline__ uint64_t num_tiles() {
   return ((uint64_t)gridDim.x * blockDim.x) / W;
 }
 
+// Loop condition of every tile loop below: true while any tile of the calling warp has work, so
+// that all lanes of the warp meet here once per iteration. Tiles of one warp that diverge (one
+// waits on a lock while the other copies a node) otherwise drift apart and issue their
+// instructions one tile at a time; met once per op they issue together and overlap their memory
+// round trips. A tile without work in an iteration skips its body. Block sizes are multiples of
+// 32, and no lane returns from inside such a loop.
+__device__ __forceinline__ bool warp_any(bool more) { return __any_sync(0xffffffffu, more); }
+
 template <int W, bool kStrong>
 __global__ void __launch_bounds__(256) k_find(device_tree T, const uint32_t* __restrict__ keys,
                                               uint32_t* __restrict__ out, uint32_t n, uint32_t ts) {
   auto tile = cg::tiled_partition<W>(cg::this_thread_block());
-  for (uint64_t i = first_tile<W>(); i < n; i += num_tiles<W>()) {
+  for (uint64_t i = first_tile<W>(); warp_any(i < n); i += num_tiles<W>()) {
+    if (i >= n) continue;
     uint32_t key = keys[i];
     uint32_t v   = kStrong ? T.cooperative_find<W>(key, tile, ts, true) : T.find_quiescent<W>(key, tile, ts);
     if (tile.thread_rank() == 0) out[i] = v;
@@ -146,7 +155,8 @@ template <int W>
 __global__ void __launch_bounds__(256) k_insert(device_tree T, const uint32_t* __restrict__ keys,
                                                 const uint32_t* __restrict__ values, uint32_t n) {
   auto tile = cg::tiled_partition<W>(cg::this_thread_block());
-  for (uint64_t i = first_tile<W>(); i < n; i += num_tiles<W>()) {
+  for (uint64_t i = first_tile<W>(); warp_any(i < n); i += num_tiles<W>()) {
+    if (i >= n) continue;
     uint32_t key = keys[i], value = values[i];
     uint32_t E   = T.versioned ? T.current_epoch() : 0u;
     T.cooperative_insert<W>(key, value, tile, E);
@@ -157,7 +167,8 @@ template <int W>
 __global__ void __launch_bounds__(256) k_erase(device_tree T, const uint32_t* __restrict__ keys,
                                                uint32_t n) {
   auto tile = cg::tiled_partition<W>(cg::this_thread_block());
-  for (uint64_t i = first_tile<W>(); i < n; i += num_tiles<W>()) {
+  for (uint64_t i = first_tile<W>(); warp_any(i < n); i += num_tiles<W>()) {
+    if (i >= n) continue;
     uint32_t key = keys[i];
     uint32_t E   = T.versioned ? T.current_epoch() : 0u;
     T.cooperative_erase<W>(key, tile, E);
@@ -170,7 +181,8 @@ __global__ void __launch_bounds__(256) k_range(device_tree T, const uint32_t* __
                                                uint32_t* counts, uint32_t avg_len, uint32_t n,
                                                uint32_t ts) {
   auto tile = cg::tiled_partition<W>(cg::this_thread_block());
-  for (uint64_t i = first_tile<W>(); i < n; i += num_tiles<W>()) {
+  for (uint64_t i = first_tile<W>(); warp_any(i < n); i += num_tiles<W>()) {
+    if (i >= n) continue;
     uint32_t lo = lower[i], hi = upper[i];
     uint2* out  = result ? result + i * (uint64_t)avg_len : nullptr;
     uint32_t c  = T.cooperative_range_query<W>(lo, hi, tile, ts, out, avg_len, kStrong);
@@ -199,7 +211,8 @@ __global__ void __launch_bounds__(256)
   const uint32_t S     = ver ? mvbt::ld_relaxed_u32(snap_word) : mvbt::kLatest;
   const uint32_t E     = ver ? S + 1 : 0u;
   const uint64_t total = (uint64_t)n_ins + n_rq;
-  for (uint64_t i = first_tile<W>(); i < total; i += num_tiles<W>()) {
+  for (uint64_t i = first_tile<W>(); warp_any(i < total); i += num_tiles<W>()) {
+    if (i >= total) continue;
     uint64_t a, r;
     if (split_op(i, n_ins, total, a, r)) {
       T.cooperative_insert<W>(keys[a], values[a], tile, E);
@@ -221,7 +234,8 @@ __global__ void __launch_bounds__(256)
   const uint32_t S     = ver ? mvbt::ld_relaxed_u32(snap_word) : mvbt::kLatest;
   const uint32_t E     = ver ? S + 1 : 0u;
   const uint64_t total = (uint64_t)n_find + n_erase;
-  for (uint64_t i = first_tile<W>(); i < total; i += num_tiles<W>()) {
+  for (uint64_t i = first_tile<W>(); warp_any(i < total); i += num_tiles<W>()) {
+    if (i >= total) continue;
     uint64_t e, f;
     if (split_op(i, n_erase, total, e, f)) {
       T.cooperative_erase<W>(ekeys[e], tile, E);
@@ -253,7 +267,8 @@ __global__ void __launch_bounds__(256) k_find_sorted(device_tree T, const uint32
   uint64_t i, end;
   tile_run<W>(n, i, end);
   mvbt::finger<W> f;
-  for (; i < end; ++i) {
+  for (; warp_any(i < end); ++i) {
+    if (i >= end) continue;
     const uint32_t key = skeys[i];
     const uint32_t v   = kStrong ? T.cooperative_find<W>(key, tile, ts, true, f.start_for(key, tile), &f)
                                  : T.find_quiescent<W>(key, tile, ts, f.start_for(key, tile), &f);
@@ -271,7 +286,8 @@ __global__ void __launch_bounds__(256) k_range_sorted(device_tree T, const uint3
   uint64_t i, end;
   tile_run<W>(n, i, end);
   mvbt::finger<W> f;
-  for (; i < end; ++i) {
+  for (; warp_any(i < end); ++i) {
+    if (i >= end) continue;
     const uint32_t lo = slower[i], p = spos[i];
     uint2* out        = result ? result + p * (uint64_t)avg_len : nullptr;
     const uint32_t c  = T.cooperative_range_query<W>(lo, upper[p], tile, ts, out, avg_len, kStrong,
@@ -287,7 +303,7 @@ __device__ __forceinline__ bool superseded(const uint32_t* skeys, uint64_t i, ui
 }
 
 template <int W>
-__global__ void __launch_bounds__(256) k_insert_sorted(device_tree T, const uint32_t* __restrict__ skeys,
+__global__ void __launch_bounds__(256, 6) k_insert_sorted(device_tree T, const uint32_t* __restrict__ skeys,
                                                        const uint32_t* __restrict__ spos,
                                                        const uint32_t* __restrict__ values, uint32_t n) {
   auto tile        = cg::tiled_partition<W>(cg::this_thread_block());
@@ -295,7 +311,8 @@ __global__ void __launch_bounds__(256) k_insert_sorted(device_tree T, const uint
   uint64_t i, end;
   tile_run<W>(n, i, end);
   mvbt::finger<W> f;
-  while (i < end) {
+  while (warp_any(i < end)) {
+    if (i >= end) continue;
     if (superseded(skeys, i, n)) {
       ++i;
       continue;
@@ -315,7 +332,8 @@ __global__ void __launch_bounds__(256) k_insert_spread(device_tree T, const uint
                                                        uint32_t m) {
   auto tile        = cg::tiled_partition<W>(cg::this_thread_block());
   const uint32_t E = T.versioned ? T.current_epoch() : 0u;
-  for (uint64_t j = first_tile<W>(); j < m; j += num_tiles<W>()) {
+  for (uint64_t j = first_tile<W>(); warp_any(j < m); j += num_tiles<W>()) {
+    if (j >= m) continue;
     const uint64_t i = j * n / m;
     if (superseded(skeys, i, n)) continue;
     T.cooperative_insert<W>(skeys[i], values[spos[i]], tile, E);
@@ -330,7 +348,8 @@ __global__ void __launch_bounds__(256) k_erase_sorted(device_tree T, const uint3
   uint64_t i, end;
   tile_run<W>(n, i, end);
   mvbt::finger<W> f;
-  for (; i < end; ++i) T.erase_in_run<W>(skeys[i], tile, E, f);
+  for (; warp_any(i < end); ++i)
+    if (i < end) T.erase_in_run<W>(skeys[i], tile, E, f);
 }
 
 // ----------------------------------------------------------------------------------------------
