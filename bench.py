@@ -92,7 +92,38 @@ def parse_args():
                          "insert + range) reported under \"configs\"")
     ap.add_argument("--config-reps", type=int, default=2,
                     help="timed experiments per c1-c3 measurement (after one untimed)")
+    ap.add_argument("--profile-case", choices=["sorted-insert-16M"], default=None,
+                    help="run only a small case of one kernel for a profiler capture and exit: "
+                         "sorted-insert-16M = a 16M-key bulk-loaded versioned tree, a snapshot, "
+                         "then one insert call of 3.6M new keys (the u90 mix of config 3 at 0.4x)")
     return ap.parse_args()
+
+
+def run_profile_case(args) -> None:
+    """A small case of one kernel, sized for an ncu capture (about 1 GB on the device)."""
+    import torch
+    import mvgpubtree_b200 as mv
+    import workload as wl
+
+    def dev(a):
+        return torch.from_numpy(np.ascontiguousarray(a).view(np.int32)).cuda()
+
+    seed, n, m = args.seed, 16_000_000, 3_600_000
+    keys = wl.distinct_keys(seed, 0, n)
+    ins = wl.distinct_keys(seed, n, m)
+    t = mv.gpu_versioned_btree(pool_bytes=1 << 30, tile_width=args.tile_width)
+    t.insert(dev(keys), dev(wl.values_for(keys, seed)))
+    t.take_snapshot()
+    di, dv = dev(ins), dev(wl.values_for(ins, seed))
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    t.insert(di, dv)
+    b.record()
+    b.synchronize()
+    t.check_errors()
+    print(json.dumps({"case": args.profile_case, "tile_width": args.tile_width, "ms": round(a.elapsed_time(b), 3),
+                      "mops": round(m / a.elapsed_time(b) / 1e3, 1)}), flush=True)
+    t.close()
 
 
 # ------------------------------------------------------------------------------------------------
@@ -1072,6 +1103,9 @@ def reference_step_check(args, seed: int, b, gpu_result, gpu_pairs) -> dict:
 def main():
     args = parse_args()
     dist = Dist()
+    if args.profile_case:
+        run_profile_case(args)
+        return
     if args.impl == "reference":
         out = run_reference(args, dist)
         if out is not None:

@@ -302,6 +302,8 @@ struct node_regs {
 
 #if defined(MVBT_HOST_EMULATION)
 MVBT_DEV uint32_t sm_id() { return emu::sm; }
+template <class Tile>
+MVBT_DEV uint32_t tile_ordinal(const Tile&) { return emu::sm; }
 MVBT_DEV unsigned long long global_ns() {
   return (unsigned long long)std::chrono::duration_cast<std::chrono::nanoseconds>(
              std::chrono::steady_clock::now().time_since_epoch())
@@ -327,6 +329,11 @@ MVBT_DEV void st_lane(uint32_t* p, const node_regs<W>& n) {
   }
 }
 #else
+// Ordinal of the calling tile among the tiles of the launch.
+template <class Tile>
+MVBT_DEV uint32_t tile_ordinal(const Tile& t) {
+  return (blockIdx.x * blockDim.x + threadIdx.x) / t.num_threads();
+}
 MVBT_DEV uint32_t sm_id() {
   uint32_t r;
   asm volatile("mov.u32 %0, %%smid;" : "=r"(r));
@@ -1932,8 +1939,10 @@ struct batch_sched {
                                               // free_avail, stat_reclaimed (memory over time)
 };
 
-constexpr uint32_t kWriteClaim = 1;  // writes per tile per claim
-constexpr uint32_t kReadClaim  = 4;  // reads per tile per claim
+constexpr uint32_t kWriteClaim   = 1;   // writes per tile per claim
+constexpr uint32_t kAdvancers    = 16;  // one waiting tile in 16 advances the batch chain each poll
+constexpr uint32_t kAdvanceEvery = 8;   // the others on every 8th poll
+constexpr uint32_t kReadClaim    = 4;   // reads per tile per claim
 
 // Largest b in [lo, nb) with pre[b] <= x (pre is non-decreasing), starting from the hint lo.
 MVBT_DEV uint32_t batch_of_ordinal(const uint64_t* pre, uint32_t nb, uint64_t x, uint32_t lo) {
@@ -2001,10 +2010,15 @@ template <class Tile>
 MVBT_DEV bool wait_batch_ready(const device_tree& T, const batch_sched& sc, uint32_t nb, uint32_t b,
                                const Tile& t) {
   const unsigned long long t0 = global_ns();
+  // Thousands of tiles can wait here at once, and every poll reads the same few words (the batch
+  // counter and the finished batch's write count) on one L2 slice. One tile in kAdvancers tries
+  // to advance the chain on every poll, the others on every kAdvanceEvery-th and otherwise only
+  // read the counter, backing off longer, so the slice keeps up with the writers' own counting.
+  const bool advancer = tile_ordinal(t) % kAdvancers == 0;
   for (uint32_t w = 0;; ++w) {
     uint32_t d = 0;
     if (t.thread_rank() == 0) {
-      advance_done(sc, nb, T.ctl);
+      if (advancer || w % kAdvanceEvery == kAdvanceEvery - 1) advance_done(sc, nb, T.ctl);
       d = ld_relaxed_u32(sc.done_batches);
     }
     d = t.shfl(d, 0);
@@ -2014,7 +2028,7 @@ MVBT_DEV bool wait_batch_ready(const device_tree& T, const batch_sched& sc, uint
       return true;
     }
     if (wait_expired(t0, T.ctl->wait_ns, t)) return false;
-    __nanosleep(w < 8 ? 128 : 1024);
+    __nanosleep(advancer ? 128 : (w < 4 ? 256 : 2048));
   }
 }
 
@@ -2098,11 +2112,11 @@ MVBT_DEV void batched_worker(const device_tree& T, const batch_view& B, const ba
           } else {
             run_batch_op<W>(T, B, i, S0 + b, S0 + b + 1, t);
           }
-          __threadfence();
-          t.sync();
           // Counted without reading the sum back (a reduction the tile does not wait for): the
           // tiles that wait for a batch (wait_batch_ready) and the warps with nothing runnable
-          // advance done_batches.
+          // advance done_batches. No fence here: every write path ends with the fence of its
+          // last release or unlock, which orders its stores before this count.
+          t.sync();
           if (t.thread_rank() == 0) atomicAdd(&sc.writes_done[b], 1u);
         }
         // the writes just made copies: free as many older ones as there are reclaimable, so
