@@ -71,8 +71,12 @@ def parse_args():
     ap.add_argument("--tile-width", type=int, default=8)
     ap.add_argument("--blocks-per-sm", type=int, default=0,
                     help="0 = full occupancy of the default kernel; 6 / 8 = register-capped variants")
-    ap.add_argument("--e2e-steps", type=int, default=4)
-    ap.add_argument("--pool-gb", type=float, default=24.0)
+    ap.add_argument("--e2e-steps", type=int, default=12,
+                    help="timed steps of the end-to-end pipeline (two in flight; more steps amortise its fill and drain)")
+    ap.add_argument("--pool-gb", type=float, default=30.0,
+                    help="node pool of each tree of the batched, plain and e2e arms")
+    ap.add_argument("--serve-pool-gb", type=float, default=24.0,
+                    help="node pool of the serving sessions (the memory cap of config 5)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep --tile-width / --blocks-per-sm instead of tuning the launch shape")
@@ -568,8 +572,8 @@ def run_ours(args, dist: Dist):
         "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded)",
         "config": {
             "workload": "mixed batches (erase 10 %, insert 20 %, find 50 % with 50 % hits, range "
-                        "20 % with L~geometric(32) clipped [1,1024], stride 107) on a 40M-key "
-                        "versioned B-link tree, one snapshot per batch",
+                        f"20 % with L~geometric(32) clipped [1,1024], stride 107) on a "
+                        f"{args.initial_keys / 1e6:g}M-key versioned B-link tree, one snapshot per batch",
             "initial_keys": args.initial_keys, "batches_per_step": args.batches,
             "batch_size": "lognormal median 16384, sigma 1.5, clipped [1024, 4194304]",
             "mean_ops_per_step": int(mean_ops), "mode": "persistent launch, device work queue",
@@ -649,7 +653,7 @@ def run_serving(args, seed: int, init, vals, dev) -> dict:
     import mvgpubtree_b200 as mv
     import workload as wl
     loads = [float(x) for x in str(args.serve_loads).split(",") if x.strip()]
-    pool = int(args.pool_gb * (1 << 30))
+    pool = int(args.serve_pool_gb * (1 << 30))
     trees = {"batched": mv.gpu_versioned_btree(pool_bytes=pool, tile_width=args.tile_width, reclaim=True),
              "plain": mv.gpu_versioned_btree(pool_bytes=pool, tile_width=args.tile_width)}
     for t in trees.values():
@@ -682,7 +686,7 @@ def run_serving(args, seed: int, init, vals, dev) -> dict:
                     "reclamation inside every launch, admission by free nodes and by reclamation lag",
             "request_size": "lognormal median 256 ops, sigma 1.5, clipped [1, 65536]",
             "arrivals": "Poisson", "seconds_per_load": "min(serve_seconds, serve_max_ops / load)",
-            "serve_seconds": args.serve_seconds, "serve_max_ops": args.serve_max_ops, "pool_gb": args.pool_gb,
+            "serve_seconds": args.serve_seconds, "serve_max_ops": args.serve_max_ops, "pool_gb": args.serve_pool_gb,
             "per_load": per_load,
             "headline": {"offered_mops": head["offered_mops"], **{k: head["batched"][k] for k in
                          ("achieved_mops", "p50_us", "p99_us", "p999_us")}},
