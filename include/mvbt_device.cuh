@@ -50,9 +50,10 @@
 //     anchor, so no node ever changes its level or role (a reader that sees a mix of two
 //     versions of a node still follows a valid route);
 //   * versioning (versioned trees): a writer in epoch E that first touches a node whose ts < E
-//     copies it to a fresh node O, publishes the header {ts = E, older = O} before changing the
-//     data, and nodes created by splits in epoch E point to the same O. A reader at snapshot S
-//     follows `older` while ts > S, so the version it uses is immutable.
+//     copies it to a fresh node O and publishes the header {ts = E, older = O} once O is complete,
+//     and nodes created by splits in epoch E point to the same O. A reader at snapshot S follows
+//     `older` while ts > S, so the version it uses is immutable; a reader under writers validates
+//     the leaf it uses with its mod word and header read again after it (recheck_version).
 //   * every wait is bounded; on a limit the operation gives up, records an error bit in the
 //     control block and returns (no trap, no unbounded loop).
 #pragma once
@@ -957,12 +958,14 @@ struct device_tree {
       hc.mod         = kRetiredBit | (E & kCountMask);  // immutable; read only at snapshots < E
       set_header<W>(c, hc, t);
       store<W>(copy, c, t);
-      publish_fence(t);
+      publish_fence(t);  // the copy is complete before the header names it
       h.ts = E;
       h.ol = (h.ol & ~kIndexMask) | copy;
       set_header<W>(n, h, t);
       store_header<W>(idx, n, t);
-      publish_fence(t);
+      // No fence between the header and the data change: a snapshot reader that saw data of this
+      // change before the header finds the mod word changed (the lock preceded every store here)
+      // and reads the leaf again (recheck_version); the release's fence publishes both.
       if (t.thread_rank() == 0) retire(copy);
     }
     return true;
@@ -1060,10 +1063,6 @@ struct device_tree {
     return true;
   }
 
-  // A concurrent snapshot reader that is about to use the data of a leaf version it read with
-  // ts <= snapshot re-reads the header after a fence. A writer publishes {ts = E, older = copy}
-  // before it changes the data, so if any lane saw changed data the re-read shows ts > snapshot:
-  // the reader then returns the index of the immutable copy (else kNone: the data is consistent).
   // Reads leaf idx for a reader of the newest state while writers may run: a sequence lock on
   // the mod word (lock bit | count). A writer holds the lock bit while it changes a reachable
   // leaf and clears it with a bumped count in one exchange after its stores, so the data is
@@ -1095,16 +1094,33 @@ struct device_tree {
     return false;
   }
 
+  // A concurrent snapshot reader that is about to use the data of a leaf version it read with
+  // ts <= snapshot re-reads the leaf's mod word and header after a fence (mod0 = the mod word of
+  // the read itself). Returns the immutable copy to read instead if the header now shows a version
+  // newer than the snapshot (a writer publishes {ts = E, older = copy} only after the copy is
+  // complete). Otherwise sets retry if the mod word was locked or has changed: a writer locked the
+  // leaf before any of its stores, so data of a change the header does not show yet can only have
+  // been read while the word differs. Returns kNone with retry false if the data read is the
+  // version at ts: no writer changed the leaf since before the read, or one did and released it
+  // before the mod word was read, whose release fence also published its header (then ts2 > ts).
   template <class Tile>
-  MVBT_DEV uint32_t recheck_version(uint32_t idx, uint32_t ts, const Tile& t) const {
+  MVBT_DEV uint32_t recheck_version(uint32_t idx, uint32_t ts, uint32_t mod0, bool& retry,
+                                    const Tile& t) const {
     __threadfence();
     t.sync();
     unsigned long long v = 0;
-    if (t.thread_rank() == 0)
-      v = ld_relaxed_u64(reinterpret_cast<const unsigned long long*>(node_ptr(idx) + 30));
+    uint32_t mod1        = 0;
+    if (t.thread_rank() == 0) {
+      mod1 = ld_relaxed_u32(node_ptr(idx) + kModWord);
+      v    = ld_relaxed_u64(reinterpret_cast<const unsigned long long*>(node_ptr(idx) + 30));
+    }
     v            = t.shfl(v, 0);
+    mod1         = t.shfl(mod1, 0);
     uint32_t ts2 = (uint32_t)v, ol2 = (uint32_t)(v >> 32);
-    return ts2 > ts ? (ol2 & kIndexMask) : kNone;
+    retry        = false;
+    if (ts2 > ts) return ol2 & kIndexMask;
+    retry = (mod0 & kLockBit) != 0 || mod1 != mod0;
+    return kNone;
   }
 
   // ------------------------------------------------------------------------------------------
@@ -1146,10 +1162,15 @@ struct device_tree {
       }
       if (h.is_leaf()) {
         if (snap && concurrent && !copy) {
-          uint32_t older = recheck_version(idx, ts, t);
+          bool retry     = false;
+          uint32_t older = recheck_version(idx, ts, h.mod, retry, t);
           if (older != kNone) {  // changed under us: use the immutable copy instead
             idx       = older;
             via_older = true;
+            continue;
+          }
+          if (retry) {  // a writer is changing it: read it again (bounded by the step limit)
+            __nanosleep(64);
             continue;
           }
         } else if (seqlk && !stable) {
@@ -1260,10 +1281,15 @@ struct device_tree {
       }
       if (h.is_leaf()) {
         if (snap && concurrent && !copy) {
-          uint32_t older = recheck_version(idx, ts, t);
+          bool retry     = false;
+          uint32_t older = recheck_version(idx, ts, h.mod, retry, t);
           if (older != kNone) {
             idx       = older;
             via_older = true;
+            continue;
+          }
+          if (retry) {
+            __nanosleep(64);
             continue;
           }
         } else if (seqlk && !stable) {
@@ -1327,10 +1353,15 @@ struct device_tree {
         via_older = false;
         if (snap && !to_version<W>(idx, n, h, ts, concurrent, copy, t)) return count;
         if (snap && concurrent && !copy) {
-          uint32_t older = recheck_version(idx, ts, t);
+          bool retry     = false;
+          uint32_t older = recheck_version(idx, ts, h.mod, retry, t);
           if (older != kNone) {
             idx       = older;
             via_older = true;
+            continue;
+          }
+          if (retry) {
+            __nanosleep(64);
             continue;
           }
         }
