@@ -887,6 +887,7 @@ def run_configs_ours(args) -> dict:
         t.close()
     del d_sk, d_sv
     w = max(runs, key=lambda k: _hmean(list(runs[k].values())))
+    ws = max(seq, key=lambda k: _hmean(list(seq[k].values())))
     wi = max(insert_mops, key=insert_mops.get)
     bad = sum(sum(x for k, v in ch.items() if k.endswith("_bad") for x in v) for ch in checks.values())
     out["c3_insert_range_40M"] = {
@@ -895,7 +896,10 @@ def run_configs_ours(args) -> dict:
         "insert_40M_per_op_mops_by_width": insert_per_op,
         "frontend": "auto (the 40M-key tree is a bulk load; the mixes sort their calls)",
         "concurrent_mops": runs[w], "concurrent_hmean_mops": round(_hmean(list(runs[w].values())), 1),
-        "sequence_mops": seq[w], "sequence_hmean_mops": round(_hmean(list(seq[w].values())), 1),
+        "sequence_tile_width": ws,
+        "sequence_mops": seq[ws], "sequence_hmean_mops": round(_hmean(list(seq[ws].values())), 1),
+        "hmean_by_width": {str(x): {"concurrent": round(_hmean(list(runs[x].values())), 1),
+                                    "sequence": round(_hmean(list(seq[x].values())), 1)} for x in runs},
         "verified": bad == 0,
         "check": {"how": "every range count and every pair min(count, 2L) of every query, both tile "
                          "widths, concurrent and sequence forms, against the oracle's state at the "
