@@ -614,8 +614,18 @@ def run_ours(args, dist: Dist):
     trees.clear()
     torch.cuda.empty_cache()
     if args.serve_loads:
-        out["serving"] = run_serving(args, seed, init, vals, dev)
+        out["serving"] = run_serving(args, seed, init, vals, dev,
+                                     verify=dist.world == 1 and not args.no_cpu_baseline)
         out["serving_p99_us"] = out["serving"]["headline"]["p99_us"]
+        checks = [r["batched"]["oracle_check"] for r in out["serving"]["per_load"] if "oracle_check" in r["batched"]]
+        if checks:
+            out["verified"]["serving_vs_oracle"] = {
+                "identical": all(c["identical"] for c in checks),
+                "results_compared": sum(c["results_compared"] for c in checks),
+                "pairs_compared": sum(c["pairs_compared"] for c in checks),
+                "how": "every batched serving session replayed on the partitioned oracle: the requests "
+                       "that share a snapshot as one batch, in snapshot order, carrying the state across "
+                       "the offered loads; every find value, range count and range pair compared"}
     return out, plain, (init, vals, steps[0], step0)
 
 
@@ -644,11 +654,14 @@ def latency_summary(arrival_ns, done_ns, ops: int) -> dict:
             "p999_us": round(float(np.percentile(lat, 99.9)), 1), "max_us": round(float(lat.max()), 1)}
 
 
-def run_serving(args, seed: int, init, vals, dev) -> dict:
+def run_serving(args, seed: int, init, vals, dev, verify: bool = True) -> dict:
     """Serving (continuous batching) at each offered load: Poisson arrivals of mixed requests
     (lognormal sizes, median 256 ops, clipped [1, 64K]) for args.serve_seconds, on a 40M-key tree
     with reclamation; beside it the plain mode (one request per launch) on an identical tree.
-    Latency = arrival to results on the host; throughput = ops / (start to last completion)."""
+    Latency = arrival to results on the host; throughput = ops / (start to last completion).
+    Every result of the batched sessions is replayed on the partitioned oracle (verify=True): the
+    requests that share a snapshot form one batch, applied in snapshot order, and every find value,
+    range count and range pair is compared."""
     import torch
     import mvgpubtree_b200 as mv
     import workload as wl
@@ -659,6 +672,11 @@ def run_serving(args, seed: int, init, vals, dev) -> dict:
     for t in trees.values():
         t.insert(dev(init), dev(vals))
         t.check_errors()
+    replay = None
+    if verify:
+        import oracle
+        replay = oracle.PartitionedMVMap(os.cpu_count() or 1, versioned=True)
+        replay.insert(init, vals)
     gen = wl.serving_generator(seed, args.initial_keys, wl.stride_for(KEYS_40M))  # the trees' key set
     mean_size = 657.0  # mean of the request-size distribution (lognormal median 256, sigma 1.5)
     per_load = []
@@ -675,12 +693,16 @@ def run_serving(args, seed: int, init, vals, dev) -> dict:
             summ = latency_summary(arrival, o["done_ns"], b.num_ops)
             summ.update({k: o["stats"][k] for k in ("launches", "reclaims", "max_waiting", "memory_waits",
                                                      "max_reclaim_lag", "lag_waits", "nodes_high_water")})
+            if name == "batched" and replay is not None:
+                summ["oracle_check"] = serving_replay_check(replay, wl, b, o)
             res[name] = summ
         per_load.append(res)
     st = trees["batched"].stats()
     use = trees["batched"].compute_memory_usage()
     head = next((r for r in per_load if r["offered_mops"] == 50.0), per_load[-1])
     gen.close()
+    if replay is not None:
+        replay.close()
     return {"mode": "continuous batching: the requests that arrived while the previous launch ran "
                     "form the next launch, one snapshot per admitted batch (reads at it, writes after), "
                     "reclamation inside every launch, admission by free nodes and by reclamation lag",
@@ -692,6 +714,27 @@ def run_serving(args, seed: int, init, vals, dev) -> dict:
                          ("achieved_mops", "p50_us", "p99_us", "p999_us")}},
             "reclaimed_nodes": st["reclaimed"], "reused_nodes": st["reused"],
             "nodes_high_water": use["nodes_allocated"]}
+
+
+def serving_replay_check(m, wl, b, o) -> dict:
+    """The batched serving session `o` over trace `b` replayed on the partitioned oracle `m` (which
+    holds the tree's state before the session): requests that share a snapshot are one batch."""
+    snaps = o["snapshot"].astype(np.int64)
+    R = snaps.size
+    steps = np.diff(snaps)
+    ordered = bool(np.all((steps == 0) | (steps == 1)))
+    starts = np.concatenate([[0], np.nonzero(steps)[0] + 1, [R]])
+    g = wl.Batches(b.batch_off[starts].astype(np.uint64), b.type, b.key, b.arg, b.out_off, b.range_cap,
+                   b.range_pairs)
+    res, out = m.run_batches(g, with_pairs=True)
+    r = b.type == 3
+    take = np.minimum(res[r], b.range_cap[r]).astype(np.int64)
+    pos = np.repeat(b.out_off[r].astype(np.int64) - (np.cumsum(take) - take), take) + np.arange(int(take.sum()))
+    bad_res = int(np.count_nonzero(res != o["result"][: res.size]))
+    bad_pairs = int(np.count_nonzero((out.reshape(-1, 2)[pos] != o["range_out"][pos]).any(axis=1)))
+    return {"groups": int(len(starts) - 1), "snapshots_in_order": ordered, "results_compared": int(res.size),
+            "result_mismatches": bad_res, "pairs_compared": int(pos.size), "pair_mismatches": bad_pairs,
+            "identical": ordered and bad_res == 0 and bad_pairs == 0}
 
 
 # ------------------------------------------------------------------------------------------------
@@ -1133,6 +1176,7 @@ def main():
     v = out["verified"]
     out["verified"]["all"] = bool(v["batched_vs_plain"]["identical"]
                                   and v.get("c4_step0_vs_oracle", {}).get("identical", False)
+                                  and v.get("serving_vs_oracle", {}).get("identical", True)
                                   and all(c.get("verified", False) for c in (configs or {}).values()))
     # the comparison with the plain per-batch launch and the other configs go last on the line
     if configs is not None:
