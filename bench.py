@@ -96,10 +96,13 @@ def parse_args():
                          "insert + range) reported under \"configs\"")
     ap.add_argument("--config-reps", type=int, default=2,
                     help="timed experiments per c1-c3 measurement (after one untimed)")
-    ap.add_argument("--profile-case", choices=["sorted-insert-16M"], default=None,
+    ap.add_argument("--profile-case", choices=["sorted-insert-16M", "update-find-16M"], default=None,
                     help="run only a small case of one kernel for a profiler capture and exit: "
                          "sorted-insert-16M = a 16M-key bulk-loaded versioned tree, a snapshot, "
-                         "then one insert call of 3.6M new keys (the u90 mix of config 3 at 0.4x)")
+                         "then one insert call of 3.6M new keys (the u90 mix of config 3 at 0.4x); "
+                         "update-find-16M = a 2^24-key bulk-loaded versioned tree, a snapshot, 2^22 "
+                         "updates and then 2^22 finds at the snapshot, both through the unsorted "
+                         "path (k_insert, k_find)")
     return ap.parse_args()
 
 
@@ -112,21 +115,43 @@ def run_profile_case(args) -> None:
     def dev(a):
         return torch.from_numpy(np.ascontiguousarray(a).view(np.int32)).cuda()
 
-    seed, n, m = args.seed, 16_000_000, 3_600_000
-    keys = wl.distinct_keys(seed, 0, n)
-    ins = wl.distinct_keys(seed, n, m)
-    t = mv.gpu_versioned_btree(pool_bytes=1 << 30, tile_width=args.tile_width)
-    t.insert(dev(keys), dev(wl.values_for(keys, seed)))
-    t.take_snapshot()
-    di, dv = dev(ins), dev(wl.values_for(ins, seed))
-    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    a.record()
-    t.insert(di, dv)
-    b.record()
-    b.synchronize()
+    def timed(fn):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        fn()
+        b.record()
+        b.synchronize()
+        return a.elapsed_time(b)
+
+    seed = args.seed
+    out = {"case": args.profile_case, "tile_width": args.tile_width}
+    if args.profile_case == "sorted-insert-16M":
+        n, m = 16_000_000, 3_600_000
+        keys = wl.distinct_keys(seed, 0, n)
+        ins = wl.distinct_keys(seed, n, m)
+        t = mv.gpu_versioned_btree(pool_bytes=1 << 30, tile_width=args.tile_width)
+        t.insert(dev(keys), dev(wl.values_for(keys, seed)))
+        t.take_snapshot()
+        di, dv = dev(ins), dev(wl.values_for(ins, seed))
+        ms = timed(lambda: t.insert(di, dv))
+        out.update({"ms": round(ms, 3), "mops": round(m / ms / 1e3, 1)})
+    else:
+        n, m = 1 << 24, 1 << 22
+        keys = wl.distinct_keys(seed, 0, n)
+        t = mv.gpu_versioned_btree(pool_bytes=1 << 30, tile_width=args.tile_width)
+        t.insert(dev(keys), dev(wl.values_for(keys, seed)))
+        s0 = t.take_snapshot()
+        t.set_frontend(mv.FRONTEND_UNSORTED)
+        upd = wl.shuffle(seed + 3, keys)[:m]
+        du, duv = dev(upd), dev(wl.values_for(upd, seed ^ 1))
+        q = dev(wl.shuffle(seed + 5, keys)[:m])
+        r = torch.empty(m, dtype=torch.int32, device="cuda")
+        ms_u = timed(lambda: t.insert(du, duv))
+        ms_f = timed(lambda: t.find(q, r, timestamp=s0))
+        out.update({"update_ms": round(ms_u, 3), "update_mops": round(m / ms_u / 1e3, 1),
+                    "find_ms": round(ms_f, 3), "find_mops": round(m / ms_f / 1e3, 1)})
     t.check_errors()
-    print(json.dumps({"case": args.profile_case, "tile_width": args.tile_width, "ms": round(a.elapsed_time(b), 3),
-                      "mops": round(m / a.elapsed_time(b) / 1e3, 1)}), flush=True)
+    print(json.dumps(out), flush=True)
     t.close()
 
 
