@@ -2004,7 +2004,10 @@ MVBT_DEV void advance_done(const batch_sched& sc, uint32_t nb, control_block* ct
         unsigned long long* e = sc.series + 4ull * d;
         e[0] = ld_relaxed_u32(sc.params + 1) + d + 1u;
         e[1] = ld_relaxed_u32(&ctl->bump);
-        e[2] = ld_relaxed_u64(&ctl->free_avail);
+        // a chunk taker's reservation on free_avail is undone when fewer entries are there, so
+        // the word can dip below zero for a moment: recorded as none free
+        const unsigned long long fa = ld_relaxed_u64(&ctl->free_avail);
+        e[2] = (long long)fa < 0 ? 0ull : fa;
         e[3] = ld_relaxed_u64(&ctl->stat_reclaimed);
       }
       atomicExch(&sc.tail_at[d], tail);
