@@ -567,6 +567,37 @@ MVBT_DEV uint32_t leaf_value(const node_regs<W>& n, uint32_t key, const Tile& t)
   return (mask && key != kEmptyKey) ? r : kNotFound;
 }
 
+// Range-query step on one leaf: writes the pairs of n with lo <= key < hi ascending at
+// out[count...] (those below cap; out nullable) and returns how many there are. Collective.
+template <int W, class Tile>
+MVBT_DEV uint32_t leaf_collect(const node_regs<W>& n, uint32_t lo, uint32_t hi, uint2* out, uint32_t cap,
+                               uint32_t count, const Tile& t) {
+  constexpr int P = 16 / W;
+  int first = -1, inr = 0;
+  bool in[P];
+#pragma unroll
+  for (int j = 0; j < P; ++j) {
+    const int q = pair_index<W>(t, j);
+    in[j]       = q < kDataPairs && n.k[j] != kEmptyKey && n.k[j] >= lo && n.k[j] < hi;
+    const uint32_t m = t.ballot(in[j]);
+    inr += __popc(m);
+    if (m) {
+      const int f = (__ffs(m) - 1) * P + j;
+      first       = (first < 0 || f < first) ? f : first;
+    }
+  }
+  if (out != nullptr) {
+#pragma unroll
+    for (int j = 0; j < P; ++j) {
+      if (in[j]) {
+        const uint32_t o = count + (uint32_t)(pair_index<W>(t, j) - first);
+        if (o < cap) out[o] = make_uint2(n.k[j], n.v[j]);
+      }
+    }
+  }
+  return (uint32_t)inr;
+}
+
 // Fetches pair `src` (per-lane index, 0..15) of node n. Collective.
 template <int W, class Tile>
 MVBT_DEV void fetch_pair(const node_regs<W>& n, int src, uint32_t& k, uint32_t& v, const Tile& t) {
@@ -1243,7 +1274,6 @@ struct device_tree {
   MVBT_DEV uint32_t cooperative_range_query(uint32_t lo, uint32_t hi, const Tile& t, uint32_t ts,
                                             uint2* out, uint32_t cap, bool concurrent = false,
                                             uint32_t start = kAnchor, finger<W>* f = nullptr) const {
-    constexpr int P = 16 / W;
     if (hi <= lo) return 0;
     const bool snap  = versioned && ts != kLatest;
     const bool seqlk = !snap && concurrent;  // newest state under writers (read_leaf_latest)
@@ -1310,29 +1340,7 @@ struct device_tree {
     // scan leaves to the right (a sibling chain is never longer than the pool)
     uint32_t count = 0;
     for (uint32_t leaves = 0;; ++leaves) {
-      int first = -1, inr = 0;
-      bool in[P];
-#pragma unroll
-      for (int j = 0; j < P; ++j) {
-        int q = pair_index<W>(t, j);
-        in[j] = q < kDataPairs && n.k[j] != kEmptyKey && n.k[j] >= lo && n.k[j] < hi;
-        uint32_t m = t.ballot(in[j]);
-        inr += __popc(m);
-        if (m) {
-          int f = (__ffs(m) - 1) * P + j;
-          first = (first < 0 || f < first) ? f : first;
-        }
-      }
-      if (out != nullptr) {
-#pragma unroll
-        for (int j = 0; j < P; ++j) {
-          if (in[j]) {
-            uint32_t o = count + (uint32_t)(pair_index<W>(t, j) - first);
-            if (o < cap) out[o] = make_uint2(n.k[j], n.v[j]);
-          }
-        }
-      }
-      count += inr;
+      count += leaf_collect<W>(n, lo, hi, out, cap, count, t);
       if (!(hi > h.high && h.sibling() != kNone)) break;
       if (leaves >= capacity) {
         if (t.thread_rank() == 0) set_error(kErrStepLimit, 6);
@@ -1370,6 +1378,74 @@ struct device_tree {
       if (!settled) {
         if (t.thread_rank() == 0) set_error(kErrStepLimit, 7);
         return count;
+      }
+    }
+    return count;
+  }
+
+  // The range query of a tree no writer changes meanwhile (concurrent = false): the same route
+  // and result as cooperative_range_query(lo, hi, t, ts, out, cap, false, start, f), with every
+  // lane loading the header words itself (as find_quiescent) on the descent and along the leaf
+  // chain, and the versions a snapshot read passes over read as headers alone.
+  template <int W, class Tile>
+  MVBT_DEV uint32_t range_quiescent(uint32_t lo, uint32_t hi, const Tile& t, uint32_t ts, uint2* out,
+                                    uint32_t cap, uint32_t start = kAnchor, finger<W>* f = nullptr) const {
+    if (hi <= lo) return 0;
+    const bool snap = versioned && ts != kLatest;
+    uint32_t idx    = start;
+    node_regs<W> n;
+    header h;
+    for (uint32_t step = 0;; ++step) {  // descend to the leaf that holds lo
+      if (step >= kMaxSteps) {
+        if (t.thread_rank() == 0) set_error(kErrStepLimit, 5);
+        return 0;
+      }
+      if (!valid(idx, t)) return 0;
+      h = ld_header_words(node_ptr(idx));
+      load<W>(idx, n, false, t);  // issued with the header loads
+      if (snap && h.ts > ts) {    // a newer version: move to the older one
+        idx = h.older();
+        if (idx == kNone) {
+          if (t.thread_rank() == 0) set_error(kErrCorrupt, 3);
+          return 0;
+        }
+        continue;
+      }
+      if (lo < h.low) {
+        idx = kAnchor;
+        continue;
+      }
+      if (lo >= h.high && h.sibling() != kNone) {
+        idx = h.sibling();
+        continue;
+      }
+      if (h.is_leaf()) {
+        if (f) f->record(0, idx, h.low, h.high, t);
+        break;
+      }
+      if (f) f->record(h.level(), idx, h.low, h.high, t);
+      idx = child_for<W>(n, lo, t);
+      if (idx == kNone) idx = kAnchor;
+    }
+    uint32_t count = 0;
+    for (uint32_t leaves = 0;; ++leaves) {  // scan leaves to the right
+      count += leaf_collect<W>(n, lo, hi, out, cap, count, t);
+      if (!(hi > h.high && h.sibling() != kNone)) break;
+      if (leaves >= capacity) {
+        if (t.thread_rank() == 0) set_error(kErrStepLimit, 6);
+        break;
+      }
+      idx = h.sibling();
+      for (uint32_t hops = 0;; ++hops) {  // the next leaf, at ts
+        if (!valid(idx, t)) return count;
+        h = ld_header_words(node_ptr(idx));
+        load<W>(idx, n, false, t);
+        if (!(snap && h.ts > ts)) break;
+        idx = h.older();
+        if (idx == kNone || hops >= kMaxSteps) {
+          if (t.thread_rank() == 0) set_error(kErrCorrupt, 3);
+          return count;
+        }
       }
     }
     return count;

@@ -185,7 +185,8 @@ __global__ void __launch_bounds__(256) k_range(device_tree T, const uint32_t* __
     if (i >= n) continue;
     uint32_t lo = lower[i], hi = upper[i];
     uint2* out  = result ? result + i * (uint64_t)avg_len : nullptr;
-    uint32_t c  = T.cooperative_range_query<W>(lo, hi, tile, ts, out, avg_len, kStrong);
+    uint32_t c  = kStrong ? T.cooperative_range_query<W>(lo, hi, tile, ts, out, avg_len, true)
+                          : T.range_quiescent<W>(lo, hi, tile, ts, out, avg_len);
     if (counts && tile.thread_rank() == 0) counts[i] = c;
   }
 }
@@ -290,8 +291,9 @@ __global__ void __launch_bounds__(256) k_range_sorted(device_tree T, const uint3
     if (i >= end) continue;
     const uint32_t lo = slower[i], p = spos[i];
     uint2* out        = result ? result + p * (uint64_t)avg_len : nullptr;
-    const uint32_t c  = T.cooperative_range_query<W>(lo, upper[p], tile, ts, out, avg_len, kStrong,
-                                                     f.start_for(lo, tile), &f);
+    const uint32_t c  = kStrong ? T.cooperative_range_query<W>(lo, upper[p], tile, ts, out, avg_len, true,
+                                                               f.start_for(lo, tile), &f)
+                                : T.range_quiescent<W>(lo, upper[p], tile, ts, out, avg_len, f.start_for(lo, tile), &f);
     if (counts && tile.thread_rank() == 0) counts[p] = c;
   }
 }

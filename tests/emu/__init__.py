@@ -27,7 +27,7 @@ def lib():
             "emu_insert": (None, [vp, u32p, u32p, u64, i, i]),
             "emu_erase": (None, [vp, u32p, u64, i, i]),
             "emu_find": (None, [vp, u32p, u32p, u64, u32, i, i, i]),
-            "emu_range": (None, [vp, u32p, u32p, vp, vp, u32, u64, u32, i, i]),
+            "emu_range": (None, [vp, u32p, u32p, vp, vp, u32, u64, u32, i, i, i]),
             "emu_insert_range": (None, [vp, u32p, u32p, u64, u32p, u32p, u64, vp, vp, u32, i, i]),
             "emu_find_erase": (None, [vp, u32p, u32p, u64, u32p, u64, i, i]),
             "emu_sorted_run": (None, [vp, i, u32p, u32p, vp, vp, vp, u32, u64, u32, i, i]),
@@ -99,31 +99,31 @@ class EmuTree:
         self.L.emu_find(self.h, k, out, k.size, ts, self.tiles, self.W, int(quiescent))
         return out
 
-    def range(self, lo, hi, avg_len, ts=0xFFFFFFFF):
+    def range(self, lo, hi, avg_len, ts=0xFFFFFFFF, quiescent=False):
         lo, hi = _u32(lo), _u32(hi)
         n = lo.size
         pairs = np.full((n, avg_len, 2), 0xFFFFFFFF, np.uint32)
         counts = np.zeros(n, np.uint32)
         self.L.emu_range(self.h, lo, hi, pairs.ctypes.data, counts.ctypes.data, avg_len, n, ts,
-                         self.tiles, self.W)
+                         self.tiles, self.W, int(quiescent))
         return pairs, counts
 
     def sorted_run(self, kind: str, keys, arg=None, avg_len: int = 0, ts=0xFFFFFFFF):
         """The sorted front-end's kernels on the emulator: keys are sorted here (a stable sort, so a
         repeated key keeps its input order), each tile runs a contiguous share with its path
-        memory, results come back in input order. kind: find | range | insert | erase | qfind (the
-        find of a tree no writer changes meanwhile)."""
+        memory, results come back in input order. kind: find | range | insert | erase | qfind | qrange
+        (the find and range query of a tree no writer changes meanwhile)."""
         k = _u32(keys)
         order = np.argsort(k, kind="stable").astype(np.uint32)
         sk = np.ascontiguousarray(k[order])
-        code = {"find": 0, "range": 1, "insert": 2, "erase": 3, "qfind": 4}[kind]
+        code = {"find": 0, "range": 1, "insert": 2, "erase": 3, "qfind": 4, "qrange": 5}[kind]
         a = _u32(arg) if arg is not None else None
         out = np.zeros(k.size, np.uint32)
-        pairs = np.full((max(1, k.size), max(1, avg_len), 2), 0xFFFFFFFF, np.uint32) if kind == "range" else None
+        pairs = np.full((max(1, k.size), max(1, avg_len), 2), 0xFFFFFFFF, np.uint32) if kind in ("range", "qrange") else None
         self.L.emu_sorted_run(self.h, code, sk, order, a.ctypes.data if a is not None else None,
                               out.ctypes.data, pairs.ctypes.data if pairs is not None else None, avg_len,
                               k.size, ts, self.tiles, self.W)
-        if kind == "range":
+        if kind in ("range", "qrange"):
             return pairs[: k.size], out
         return out
 

@@ -223,14 +223,16 @@ void emu_find(void* h, const uint32_t* keys, uint32_t* out, uint64_t n, uint32_t
   }));
 }
 
+// quiescent != 0: the range query of a tree no writer changes meanwhile (range_quiescent).
 void emu_range(void* h, const uint32_t* lo, const uint32_t* hi, uint32_t* pairs, uint32_t* counts,
-               uint32_t avg_len, uint64_t n, uint32_t ts, int tiles, int W) {
+               uint32_t avg_len, uint64_t n, uint32_t ts, int tiles, int W, int quiescent) {
   auto* t = static_cast<emu_tree*>(h);
   auto v  = t->view();
   if (!v.versioned) ts = mvbt::kLatest;
   EMU_DISPATCH(W, run(n, tiles, kW, [&](uint64_t i, const emu_tile& tile) {
     uint2* o   = pairs ? reinterpret_cast<uint2*>(pairs) + i * (uint64_t)avg_len : nullptr;
-    uint32_t c = v.cooperative_range_query<kW>(lo[i], hi[i], tile, ts, o, avg_len, true);
+    uint32_t c = quiescent ? v.range_quiescent<kW>(lo[i], hi[i], tile, ts, o, avg_len)
+                           : v.cooperative_range_query<kW>(lo[i], hi[i], tile, ts, o, avg_len, true);
     if (counts && tile.thread_rank() == 0) counts[i] = c;
   }));
 }
@@ -260,8 +262,8 @@ void emu_insert_range(void* h, const uint32_t* keys, const uint32_t* vals, uint6
 // Sorted runs (the sorted batch front-end): keys[0, n) ascending, pos[i] = the input position of
 // keys[i]; each of `tiles` tiles takes one contiguous share of the run and keeps its path memory
 // (mvbt::finger, one per lane, as registers are on the GPU). kind: 0 find, 1 range, 2 insert (a
-// repeated key: its last occurrence wins; the keys of one leaf under one lock), 3 erase, 4 find of
-// a tree no writer changes meanwhile.
+// repeated key: its last occurrence wins; the keys of one leaf under one lock), 3 erase, 4 find and
+// 5 range of a tree no writer changes meanwhile.
 void emu_sorted_run(void* h, int kind, const uint32_t* keys, const uint32_t* pos, const uint32_t* arg,
                     uint32_t* out, uint32_t* pairs, uint32_t avg_len, uint64_t n, uint32_t ts, int tiles, int W) {
   auto* t = static_cast<emu_tree*>(h);
@@ -297,6 +299,10 @@ void emu_sorted_run(void* h, int kind, const uint32_t* keys, const uint32_t* pos
             if (kind == 4) {
               const uint32_t r = v.find_quiescent<kW>(k, tile, ts, f.start_for(k, tile), &f);
               if (tile.thread_rank() == 0) out[pos[i]] = r;
+            } else if (kind == 5) {
+              uint2* o = pairs ? reinterpret_cast<uint2*>(pairs) + pos[i] * (uint64_t)avg_len : nullptr;
+              const uint32_t c = v.range_quiescent<kW>(k, arg[pos[i]], tile, ts, o, avg_len, f.start_for(k, tile), &f);
+              if (out && tile.thread_rank() == 0) out[pos[i]] = c;
             } else if (kind == 0) {
               const uint32_t r = v.cooperative_find<kW>(k, tile, ts, true, f.start_for(k, tile), &f);
               if (tile.thread_rank() == 0) out[pos[i]] = r;

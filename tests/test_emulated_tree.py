@@ -213,10 +213,14 @@ def test_emulated_sorted_runs_match_oracle(w):
         assert np.array_equal(t.sorted_run("find", q, ts=ts), m.find(q, ts)), ts
         assert np.array_equal(t.sorted_run("qfind", q, ts=ts), m.find(q, ts)), ts
         assert np.array_equal(t.find(q, ts, quiescent=True), m.find(q, ts)), ts
-        pairs, counts = t.sorted_run("range", lo, hi, avg_len=48, ts=ts)
         ep, ec = m.range_query(lo, hi, 48, ts)
-        assert np.array_equal(counts, ec), ts
         mask = np.arange(48)[None, :] < np.minimum(ec, 48)[:, None]
+        for kind in ("range", "qrange"):
+            pairs, counts = t.sorted_run(kind, lo, hi, avg_len=48, ts=ts)
+            assert np.array_equal(counts, ec), (kind, ts)
+            assert np.array_equal(pairs[mask], ep[mask]), (kind, ts)
+        pairs, counts = t.range(lo, hi, 48, ts, quiescent=True)
+        assert np.array_equal(counts, ec), ts
         assert np.array_equal(pairs[mask], ep[mask]), ts
     rep = t.validate()
     assert rep["violations"] == 0 and rep["locked_nodes"] == 0 and rep["keys"] == m.size()
